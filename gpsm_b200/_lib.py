@@ -1,0 +1,122 @@
+"""ctypes binding of libgpsm.so (declared in include/gpsm.h).
+
+The library is the product: every matching call goes through its C ABI and
+runs on the GPU. If the shared object is missing, loading raises instead of
+falling back to anything else.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpsm.so")
+
+GPSM_OK = 0
+ERRORS = {
+    -1: "GPSM_ERR_INVALID",
+    -2: "GPSM_ERR_CUDA",
+    -3: "GPSM_ERR_NOMEM",
+    -4: "GPSM_ERR_NOT_FOUND",
+    -5: "GPSM_ERR_BUDGET",
+    -6: "GPSM_ERR_TIMEOUT",
+    -7: "GPSM_ERR_NODEV",
+    -8: "GPSM_ERR_STATE",
+}
+
+
+class GpsmError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
+
+
+_lib = None
+
+vp = C.c_void_p
+u32, u64, i32, i64, f64 = C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "gpsm_gen_er": (C.c_int, [u32, u64, u64, vp]),
+    "gpsm_gen_rmat": (C.c_int, [C.c_int, u64, f64, f64, f64, u64, vp]),
+    "gpsm_gen_labels": (C.c_int, [u32, u32, f64, u64, vp]),
+    "gpsm_csr_from_edges": (C.c_int, [u32, u64, vp, vp, vp]),
+    "gpsm_gen_query": (i64, [u32, vp, vp, vp, u32, C.c_int, f64, f64, u64, vp, vp, vp]),
+    "gpsm_last_error": (C.c_char_p, []),
+    "gpsm_init": (C.c_int, [C.c_int]),
+    "gpsm_init_ex": (C.c_int, [C.c_int, u64]),
+    "gpsm_shutdown": (C.c_int, []),
+    "gpsm_engine_create": (C.c_int, [C.c_int, u64, vp]),
+    "gpsm_engine_destroy": (C.c_int, [vp]),
+    "gpsm_graph_upload": (C.c_int, [vp, vp, vp, u32, vp]),
+    "gpsm_graph_free": (C.c_int, [vp]),
+    "gpsm_graph_info": (C.c_int, [vp, vp, vp, vp]),
+    "gpsm_match_ex": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
+    "gpsm_engine_match": (C.c_int, [vp, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
+    "gpsm_match": (C.c_int, [vp, u32, vp, u32, vp, u64, vp, vp, vp, vp]),
+    "gpsm_free": (None, [vp]),
+    "gpsm_debug_filter": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp, vp]),
+    "gpsm_match_batch": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "gpsm_flush_l2": (C.c_int, [vp, u64]),
+}
+
+GPSM_ORDER_PLAIN, GPSM_ORDER_GIVEN = 0, 1
+GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE = 1, 2
+
+
+class MatchOpts(C.Structure):
+    _fields_ = [("cap", u64), ("order_mode", i32), ("pad", i32), ("order", vp),
+                ("level_bytes", u64), ("result_rows", u64), ("flags", u32), ("pad2", u32)]
+
+
+class MatchInfo(C.Structure):
+    _fields_ = [("rows", u64), ("cols", u32), ("capped", i32), ("empty_filter", i32), ("pad", i32),
+                ("device_ms", f64), ("filter_ms", f64), ("join_ms", f64),
+                ("expand_launches", u64), ("filter_launches", u64), ("alg_bytes_join", u64),
+                ("expand_ms", f64)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("device_ms", f64), ("expand_ms", f64), ("filter_ms", f64), ("rows", u64), ("launches", u64),
+                ("expand_launches", u64), ("alg_bytes_join", u64)]
+
+
+def load(path=None):
+    """Load libgpsm.so once and declare every exported signature."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError(f"libgpsm.so not built at {p}; run gpsm_b200.build.build()")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a):
+    """Raw data pointer of a contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(vp)
+
+
+def check(code, what):
+    if code < 0:
+        msg = what
+        if _lib is not None:
+            err = _lib.gpsm_last_error()
+            if err:
+                msg = f"{what} ({err.decode(errors='replace')})"
+        raise GpsmError(int(code), msg)
+    return code
+
+
+def u32a(x):
+    return np.ascontiguousarray(x, dtype=np.uint32)

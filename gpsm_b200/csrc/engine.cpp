@@ -1,0 +1,652 @@
+// Per-query pipeline on one device-resident data graph.
+//
+// Order of work, as in Match::match (match/Match.cu:1710-1966):
+//   plan (host) -> candidate init + explore -> refinement -> final lists
+//   -> candidate edges (both directions) -> join order -> joins.
+// Differences that are design choices of this engine:
+//   - no host round trip per scan: compaction and scans keep their totals on
+//     the device; the host waits only twice before the joins (candidate
+//     counts, then candidate-edge totals) and once per join chunk;
+//   - the join runs depth-first over chunks of rows (a level is expanded only
+//     after every deeper level is empty), so intermediate tables are bounded
+//     by `level_bytes` per level instead of growing until cudaMalloc fails,
+//     while the output keeps the reference's row order;
+//   - injectivity is checked while joining, and the embedding cap stops the
+//     query after exactly `cap` rows (the first `cap` in row order).
+#include "engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <queue>
+
+namespace gpsm {
+
+bool QueryPlan::adjacent(uint32_t a, uint32_t b) const {
+  return std::binary_search(rcol.begin() + roff[a], rcol.begin() + roff[a + 1], b);
+}
+
+int QueryPlan::edge_between(uint32_t a, uint32_t b) const {
+  uint32_t x = std::min(a, b), y = std::max(a, b);
+  for (uint32_t e = 0; e < m; ++e)
+    if (efrom[e] == x && eto[e] == y) return (int)e;
+  return -1;
+}
+
+int plan_query(const DeviceGraph& g, uint32_t qn, const uint32_t* qlab, uint32_t qm, const uint32_t* qe,
+               QueryPlan& Q, std::string& err) {
+  if (qn == 0 || qlab == nullptr || (qm > 0 && qe == nullptr)) {
+    err = "empty query";
+    return GPSM_ERR_INVALID;
+  }
+  if (qn >= kMaxBack) {
+    err = "query has too many vertices (limit 127)";
+    return GPSM_ERR_INVALID;
+  }
+  Q = QueryPlan();
+  Q.n = qn;
+  Q.m = qm;
+  Q.lab.assign(qlab, qlab + qn);
+  Q.in.assign(qn, {});
+  Q.out.assign(qn, {});
+  std::vector<uint64_t> seen;
+  for (uint32_t i = 0; i < qm; ++i) {
+    uint32_t a = qe[2 * i], b = qe[2 * i + 1];
+    if (a >= qn || b >= qn) {
+      err = "query edge endpoint out of range";
+      return GPSM_ERR_INVALID;
+    }
+    if (a == b) {
+      err = "query self loop";
+      return GPSM_ERR_INVALID;
+    }
+    seen.push_back(((uint64_t)std::min(a, b) << 32) | std::max(a, b));
+    Q.out[a].push_back(b);
+    Q.in[b].push_back(a);
+  }
+  std::sort(seen.begin(), seen.end());
+  if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) {
+    err = "parallel query edges";
+    return GPSM_ERR_INVALID;
+  }
+  Q.roff.assign(qn + 1, 0);
+  for (uint32_t i = 0; i < qn; ++i) Q.roff[i + 1] = Q.roff[i] + (uint32_t)(Q.in[i].size() + Q.out[i].size());
+  Q.rcol.resize(Q.roff[qn]);
+  for (uint32_t i = 0; i < qn; ++i) {
+    uint32_t p = Q.roff[i];
+    for (uint32_t x : Q.in[i]) Q.rcol[p++] = x;
+    for (uint32_t x : Q.out[i]) Q.rcol[p++] = x;
+    std::sort(Q.rcol.begin() + Q.roff[i], Q.rcol.begin() + Q.roff[i + 1]);
+  }
+  for (uint32_t i = 0; i < qn; ++i)
+    for (uint32_t a : Q.in[i]) {
+      Q.efrom.push_back(std::min(a, i));
+      Q.eto.push_back(std::max(a, i));
+    }
+  // connectivity
+  {
+    std::vector<uint8_t> vis(qn, 0);
+    std::vector<uint32_t> st{0};
+    vis[0] = 1;
+    uint32_t cnt = 1;
+    while (!st.empty()) {
+      uint32_t t = st.back();
+      st.pop_back();
+      for (uint32_t k = Q.roff[t]; k < Q.roff[t + 1]; ++k)
+        if (!vis[Q.rcol[k]]) {
+          vis[Q.rcol[k]] = 1;
+          ++cnt;
+          st.push_back(Q.rcol[k]);
+        }
+    }
+    if (cnt != qn) {
+      err = "query is not connected";
+      return GPSM_ERR_INVALID;
+    }
+  }
+  if (qm == 0) {
+    Q.order = {0};
+    return GPSM_OK;
+  }
+  // generateSpanningTree (match/Match.cu:339-429): score = degree / label
+  // frequency with the reference's float arithmetic; the first edge with the
+  // largest score sum (strict >) gives the start; BFS over sorted lists.
+  std::vector<float> score(qn);
+  for (uint32_t i = 0; i < qn; ++i) {
+    float num = (float)g.label_count(Q.lab[i]);
+    int degree = (int)(Q.in[i].size() + Q.out[i].size());
+    score[i] = (float)(((double)degree + 0.0) / (double)num);
+  }
+  float maxv = 0.0f;
+  int maxi = -1;
+  for (uint32_t i = 0; i < qm; ++i) {
+    float t = score[Q.efrom[i]] + score[Q.eto[i]];
+    if (t > maxv) {
+      maxv = t;
+      maxi = (int)i;
+    }
+  }
+  if (maxi < 0) maxi = 0;
+  uint32_t start = Q.efrom[maxi];
+  if (score[Q.eto[maxi]] > score[Q.efrom[maxi]]) start = Q.eto[maxi];
+  std::vector<uint8_t> vis(qn, 0);
+  std::queue<uint32_t> q;
+  Q.order.push_back(start);
+  vis[start] = 1;
+  q.push(start);
+  while (!q.empty()) {
+    uint32_t t = q.front();
+    q.pop();
+    for (uint32_t k = Q.roff[t]; k < Q.roff[t + 1]; ++k) {
+      uint32_t a = Q.rcol[k];
+      if (vis[a]) continue;
+      vis[a] = 1;
+      Q.order.push_back(a);
+      q.push(a);
+    }
+  }
+  return GPSM_OK;
+}
+
+std::vector<int32_t> plain_order(const QueryPlan& Q, const std::vector<uint64_t>& size_fwd, uint64_t nnz) {
+  std::vector<int32_t> pos2id;
+  if (Q.m == 0) {
+    pos2id.push_back(0);
+    return pos2id;
+  }
+  std::vector<uint8_t> vv(Q.n, 0), ve(Q.m, 0);
+  uint64_t minv = nnz + 1;
+  uint32_t minx = 0;
+  for (uint32_t i = 0; i < Q.m; ++i)
+    if (size_fwd[i] < minv) {
+      minv = size_fwd[i];
+      minx = i;
+    }
+  vv[Q.efrom[minx]] = vv[Q.eto[minx]] = 1;
+  ve[minx] = 1;
+  pos2id.push_back((int32_t)Q.efrom[minx]);
+  pos2id.push_back((int32_t)Q.eto[minx]);
+  for (uint32_t c = 1; c < Q.m; ++c) {
+    // a closed edge first (both endpoints visited); it adds no column
+    uint64_t best = nnz + 1;
+    int bx = -1;
+    for (uint32_t i = 0; i < Q.m; ++i)
+      if (!ve[i] && vv[Q.efrom[i]] && vv[Q.eto[i]] && size_fwd[i] < best) {
+        best = size_fwd[i];
+        bx = (int)i;
+      }
+    if (bx < 0) {
+      for (uint32_t i = 0; i < Q.m; ++i)
+        if (!ve[i] && (vv[Q.efrom[i]] || vv[Q.eto[i]]) && size_fwd[i] < best) {
+          best = size_fwd[i];
+          bx = (int)i;
+        }
+      if (bx < 0) break;  // cannot happen for connected queries
+      uint32_t u = Q.efrom[bx], v = Q.eto[bx];
+      pos2id.push_back((int32_t)(vv[u] ? v : u));
+    }
+    vv[Q.efrom[bx]] = vv[Q.eto[bx]] = 1;
+    ve[bx] = 1;
+  }
+  return pos2id;
+}
+
+bool valid_order(const QueryPlan& Q, const std::vector<int32_t>& pos2id) {
+  if (pos2id.size() != Q.n) return false;
+  std::vector<uint8_t> seen(Q.n, 0);
+  for (size_t i = 0; i < pos2id.size(); ++i) {
+    int32_t u = pos2id[i];
+    if (u < 0 || (uint32_t)u >= Q.n || seen[u]) return false;
+    if (i > 0) {
+      bool any = false;
+      for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) any |= seen[Q.rcol[k]] != 0;
+      if (!any) return false;
+    }
+    seen[u] = 1;
+  }
+  return true;
+}
+
+namespace {
+
+template <class T>
+T* arena_alloc(Workspace& ws, uint64_t count) {
+  void* p = ws.arena.alloc(std::max<uint64_t>(count, 1) * sizeof(T));
+  if (!p) throw CudaError{cudaErrorMemoryAllocation, "arena"};
+  return (T*)p;
+}
+
+struct Level {
+  uint32_t* buf = nullptr;
+  uint64_t cap_rows = 0;
+  uint64_t nrows = 0;
+  uint64_t next = 0;
+  double ratio = 4.0;  // observed outputs per input row of the last launch
+};
+
+}  // namespace
+
+int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R) {
+  R = MatchResult();
+  const uint32_t qn = Q.n, W = g.words;
+  cudaStream_t s = ws.stream;
+  if (ws.dirty) {
+    // an earlier query stopped part-way: re-read the scan ticket counter so
+    // the host's per-launch ticket base matches the device again
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    GPSM_CUDA(cudaMemcpy(&ws.scan.ticket_base, ws.scan.d_ticket, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  }
+  ws.dirty = true;
+  ws.arena.reset();
+  R.cols = qn;
+  GPSM_CUDA(cudaEventRecord(ws.ev0, s));
+  GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, 64 * sizeof(uint32_t), s));
+
+  // ---- allocations ---------------------------------------------------------
+  uint32_t* bm = arena_alloc<uint32_t>(ws, (uint64_t)qn * W);
+  uint32_t* rank = arena_alloc<uint32_t>(ws, (uint64_t)qn * W);
+  uint32_t* counts = arena_alloc<uint32_t>(ws, qn);
+  std::vector<uint32_t*> list(qn);
+  std::vector<uint32_t> bound(qn);
+  for (uint32_t u = 0; u < qn; ++u) {
+    bound[u] = (uint32_t)g.label_count(Q.lab[u]);
+    if (bound[u] == 0) {  // a label absent from the data graph: no candidate
+      R.empty_filter = true;
+      R.id2pos.assign(qn, -1);
+      R.pos2id.assign(qn, -1);
+      return GPSM_OK;
+    }
+    list[u] = arena_alloc<uint32_t>(ws, bound[u]);
+  }
+  GPSM_CUDA(cudaMemsetAsync(bm, 0, sizeof(uint32_t) * (uint64_t)qn * W, s));
+
+  // query structure for the filter kernels: explore targets (v, label,
+  // degree) per order position, refinement targets per simple vertex
+  std::vector<uint32_t> params;
+  std::vector<uint32_t> exp_off(qn + 1, 0), exp_cnt(qn, 0);
+  std::vector<uint8_t> initialized(qn, 0);
+  {
+    std::vector<uint8_t> init_sim(qn, 0);
+    for (uint32_t i = 0; i < Q.order.size(); ++i) {
+      uint32_t u = Q.order[i];
+      init_sim[u] = 1;
+      exp_off[i] = (uint32_t)params.size();
+      for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) {
+        uint32_t v = Q.rcol[k];
+        if (!init_sim[v]) {
+          params.push_back(v);
+          params.push_back(Q.lab[v]);
+          params.push_back(Q.deg(v));
+          exp_cnt[i]++;
+        }
+      }
+      for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) init_sim[Q.rcol[k]] = 1;
+    }
+  }
+  // generateSimplifiedGraph (match/Match.cu:721-759): degree > 1
+  std::vector<uint32_t> simple;
+  std::vector<uint8_t> valid(qn, 0);
+  for (uint32_t i = 0; i < qn; ++i)
+    if (Q.deg(i) > 1) {
+      valid[i] = 1;
+      simple.push_back(i);
+    }
+  std::vector<uint32_t> ref_off(simple.size()), ref_cnt(simple.size());
+  for (size_t i = 0; i < simple.size(); ++i) {
+    ref_off[i] = (uint32_t)params.size();
+    for (uint32_t x : Q.in[simple[i]])
+      if (valid[x]) params.push_back(x), ref_cnt[i]++;
+    for (uint32_t x : Q.out[simple[i]])
+      if (valid[x]) params.push_back(x), ref_cnt[i]++;
+  }
+  uint32_t* d_params = arena_alloc<uint32_t>(ws, params.size() + 1);
+  if (!params.empty())
+    GPSM_CUDA(cudaMemcpyAsync(d_params, params.data(), params.size() * 4, cudaMemcpyHostToDevice, s));
+  GPSM_CUDA(cudaStreamSynchronize(s));  // params is pageable host memory
+
+  auto bm_of = [&](uint32_t u) { return bm + (size_t)u * W; };
+  uint64_t launches = 0;
+
+  // ---- candidate initialisation (match/Match.cu:661-719) ---------------------
+  for (uint32_t i = 0; i < Q.order.size(); ++i) {
+    const uint32_t u = Q.order[i];
+    if (!initialized[u]) {
+      uint32_t b, e;
+      g.label_range(Q.lab[u], Q.deg(u), &b, &e);
+      launch_mark_range(ws, g, b, e, bm_of(u));
+      ++launches;
+      initialized[u] = 1;
+    }
+    launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true);
+    ++launches;
+    if (exp_cnt[i]) {
+      launch_explore(ws, g, list[u], counts + u, bound[u], u, d_params + exp_off[i], exp_cnt[i], bm);
+      ++launches;
+    }
+    for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) initialized[Q.rcol[k]] = 1;
+  }
+  // ---- refinement: 4 rounds + 1 emptiness check (match/Match.cu:848-890) ----
+  for (int k = 0; k < 5; ++k)
+    for (size_t i = 0; i < simple.size(); ++i) {
+      const uint32_t u = simple[i];
+      launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true);
+      ++launches;
+      if (k == 4 || ref_cnt[i] == 0) continue;
+      launch_refine(ws, g, list[u], counts + u, bound[u], u, d_params + ref_off[i], ref_cnt[i], bm);
+      ++launches;
+    }
+  // ---- final candidate lists with ranks -----------------------------------
+  for (uint32_t u = 0; u < qn; ++u) {
+    launch_compact(ws, bm_of(u), W, list[u], rank + (size_t)u * W, counts + u, true);
+    ++launches;
+  }
+  GPSM_CUDA(cudaMemcpyAsync(ws.h_small, counts, qn * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 64, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GPSM_CUDA(cudaStreamSynchronize(s));
+  R.stats.filter_launches = launches;
+  std::vector<uint32_t> cnt(qn);
+  memcpy(cnt.data(), ws.h_small, qn * sizeof(uint32_t));
+  const uint32_t flags = *reinterpret_cast<uint32_t*>(ws.h_small + 64);
+  R.stats.cand_count = cnt;
+  if (flags & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {
+    set_last_error("device wait limit or bounds check tripped in the filter");
+    return GPSM_ERR_TIMEOUT;
+  }
+  if (flags & DF_EMPTY) {
+    R.empty_filter = true;
+    R.id2pos.assign(qn, -1);
+    R.pos2id.assign(qn, -1);
+    GPSM_CUDA(cudaEventRecord(ws.ev1, s));
+    GPSM_CUDA(cudaEventSynchronize(ws.ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ws.ev0, ws.ev1);
+    R.stats.device_ms = ms;
+    return GPSM_OK;
+  }
+
+  // ---- candidate edges, both directions (match/Match.cu:1082-1139) ----------
+  const uint32_t m = Q.m;
+  const uint32_t ndir = 2 * m;
+  std::vector<CedgeDir> dirs(ndir);
+  uint64_t items = 0;
+  for (uint32_t e = 0; e < m; ++e)
+    for (int r = 0; r < 2; ++r) {
+      uint32_t u = r ? Q.eto[e] : Q.efrom[e];
+      uint32_t v = r ? Q.efrom[e] : Q.eto[e];
+      CedgeDir& d = dirs[2 * e + r];
+      d.ids = list[u];
+      d.n = cnt[u];
+      d.v = v;
+      d.item_base = items;
+      items += cnt[u];
+    }
+  unsigned long long* goff = nullptr;
+  uint32_t* nbrs = nullptr;
+  uint64_t nbrs_total = 0;
+  std::vector<uint64_t> dir_total(ndir, 0);
+  if (ndir > 0) {
+    CedgeDir* d_dirs = arena_alloc<CedgeDir>(ws, ndir);
+    uint32_t* ccount = arena_alloc<uint32_t>(ws, items);
+    goff = arena_alloc<unsigned long long>(ws, items + 1);
+    unsigned long long* d_idx = arena_alloc<unsigned long long>(ws, ndir + 1);
+    std::vector<unsigned long long> idx(ndir + 1);
+    for (uint32_t d = 0; d < ndir; ++d) idx[d] = dirs[d].item_base;
+    idx[ndir] = items;
+    GPSM_CUDA(cudaMemcpyAsync(d_dirs, dirs.data(), ndir * sizeof(CedgeDir), cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaMemcpyAsync(d_idx, idx.data(), (ndir + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+    launch_cedge_count(ws, g, d_dirs, ndir, d_idx, items, bm, ccount);
+    launch_scan_u32(ws, ccount, items, goff);
+    launch_gather_u64(ws, goff, d_idx, ndir + 1, ws.d_small);
+    GPSM_CUDA(cudaMemcpyAsync(ws.h_small, ws.d_small, (ndir + 1) * sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4000, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    if (*reinterpret_cast<uint32_t*>(ws.h_small + 4000) & DF_SCAN_TIMEOUT) {
+      set_last_error("device wait limit tripped in candidate-edge scan");
+      return GPSM_ERR_TIMEOUT;
+    }
+    for (uint32_t d = 0; d < ndir; ++d) dir_total[d] = ws.h_small[d + 1] - ws.h_small[d];
+    const uint64_t total = ws.h_small[ndir];
+    nbrs_total = total;
+    nbrs = arena_alloc<uint32_t>(ws, total);
+    launch_cedge_write(ws, g, d_dirs, ndir, d_idx, items, bm, goff, nbrs);
+    launches += 4;
+  }
+  R.stats.size_fwd.resize(m);
+  R.stats.size_rev.resize(m);
+  for (uint32_t e = 0; e < m; ++e) {
+    R.stats.size_fwd[e] = dir_total[2 * e];
+    R.stats.size_rev[e] = dir_total[2 * e + 1];
+  }
+
+  // ---- join order -------------------------------------------------------------
+  std::vector<int32_t> pos2id;
+  if (opt.order_mode == ORDER_GIVEN) {
+    if (!valid_order(Q, opt.given_order)) {
+      set_last_error("given join order is not a connected permutation of the query vertices");
+      return GPSM_ERR_INVALID;
+    }
+    pos2id = opt.given_order;
+  } else {
+    pos2id = plain_order(Q, R.stats.size_fwd, g.nnz);
+  }
+  R.pos2id = pos2id;
+  R.id2pos.assign(qn, -1);
+  for (uint32_t p = 0; p < qn; ++p) R.id2pos[pos2id[p]] = (int32_t)p;
+  GPSM_CUDA(cudaEventRecord(ws.evm, s));
+  if (opt.filter_only) {
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    return GPSM_OK;
+  }
+
+  // ---- joins ---------------------------------------------------------------------
+  // back-neighbour descriptors for each added position p >= 1
+  std::vector<BackNbr> hb;
+  std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
+  for (uint32_t p = 1; p < qn; ++p) {
+    back_off[p] = (uint32_t)hb.size();
+    const uint32_t v = (uint32_t)pos2id[p];
+    for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
+      const uint32_t w = Q.rcol[k];
+      if ((uint32_t)R.id2pos[w] >= p) continue;
+      const int e = Q.edge_between(w, v);
+      const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
+      BackNbr b;
+      b.col = (uint32_t)R.id2pos[w];
+      b.pad = 0;
+      b.bm = bm_of(w);
+      b.rank = rank + (size_t)w * W;
+      b.off = goff + dirs[d].item_base;
+      b.nbrs = nbrs;
+      hb.push_back(b);
+      back_cnt[p]++;
+    }
+  }
+  BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
+  if (!hb.empty())
+    GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
+  ExpandResult* d_res = arena_alloc<ExpandResult>(ws, 1);
+  ExpandResult* h_res = reinterpret_cast<ExpandResult*>(ws.h_small + 1024);
+  ExpandResult* h_init = reinterpret_cast<ExpandResult*>(ws.h_small + 1032);
+  GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
+
+  R.stats.level_rows.assign(qn + 1, 0);
+  const uint64_t cap = opt.cap;
+  // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
+  std::vector<Level> L(qn + 1);
+  L[1].buf = list[pos2id[0]];
+  L[1].nrows = cnt[pos2id[0]];
+  L[1].cap_rows = L[1].nrows;
+  R.stats.level_rows[1] = L[1].nrows;
+  const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+  for (uint32_t w = 2; w < qn; ++w) {
+    uint64_t rows = std::max<uint64_t>(opt.level_bytes / (4ull * w), min_rows);
+    L[w].cap_rows = rows;
+    L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
+  }
+  uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
+  if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
+  uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
+  uint64_t res_used = 0, emitted = 0;
+  bool capped = false;
+
+  auto flush = [&]() {
+    if (!opt.collect_rows || res_used == 0) {
+      res_used = 0;
+      return;
+    }
+    size_t old = R.host_rows.size();
+    R.host_rows.resize(old + res_used * qn);
+    GPSM_CUDA(cudaMemcpyAsync(R.host_rows.data() + old, res_buf, res_used * qn * 4, cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    res_used = 0;
+  };
+
+  if (qn == 1) {
+    // single-vertex query: every candidate is an embedding
+    const uint64_t n1 = std::min<uint64_t>(L[1].nrows, cap);
+    capped = L[1].nrows >= cap;
+    if (n1 > 0)
+      GPSM_CUDA(cudaMemcpyAsync(res_buf, L[1].buf, std::min(n1, res_cap) * 4, cudaMemcpyDeviceToDevice, s));
+    if (n1 > res_cap) {
+      if (opt.keep_on_device) {
+        set_last_error("device result buffer full");
+        return GPSM_ERR_BUDGET;
+      }
+      if (opt.collect_rows) {
+        R.host_rows.resize(n1);
+        GPSM_CUDA(cudaMemcpyAsync(R.host_rows.data(), L[1].buf, n1 * 4, cudaMemcpyDeviceToHost, s));
+        GPSM_CUDA(cudaStreamSynchronize(s));
+      }
+    } else {
+      res_used = n1;
+    }
+    emitted = n1;
+    R.stats.level_rows[1] = n1;
+  }
+  uint64_t exp_launches = 0, driver_elems = 0;
+  uint64_t alg_bytes = 0;
+  while (qn > 1 && !capped) {
+    // deepest level with rows left
+    int lv = -1;
+    for (int w = (int)qn - 1; w >= 1; --w)
+      if (L[w].next < L[w].nrows) {
+        lv = w;
+        break;
+      }
+    if (lv < 0) break;
+    Level& A = L[lv];
+    const bool final_level = (uint32_t)lv + 1 == qn;
+    uint32_t* out;
+    uint64_t out_cap;
+    bool partial = false;
+    if (final_level) {
+      uint64_t space = res_cap - res_used;
+      if (space == 0) {
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        flush();
+        space = res_cap;
+      }
+      out = res_buf + res_used * qn;
+      if (cap - emitted <= space) {
+        out_cap = cap - emitted;
+        partial = true;
+      } else {
+        out_cap = space;
+      }
+    } else {
+      Level& B = L[lv + 1];
+      B.nrows = 0;
+      B.next = 0;
+      out = B.buf;
+      out_cap = B.cap_rows;
+    }
+    uint64_t want = (uint64_t)((double)out_cap / std::max(A.ratio, 1.0 / 64.0));
+    want = std::max<uint64_t>(want, 64);
+    want = std::min<uint64_t>(want, (uint64_t)ws.scan.max_tiles * 64);
+    const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
+    h_init->total = 0;
+    h_init->cut_pos = ~0ULL;
+    h_init->cut_row = ~0ULL;
+    h_init->driver = 0;
+    GPSM_CUDA(cudaMemcpyAsync(d_res, h_init, sizeof(ExpandResult), cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaEventRecord(ws.eve0, s));
+    launch_expand(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], out, out_cap, partial, d_res,
+                  nbrs_total);
+    GPSM_CUDA(cudaEventRecord(ws.eve1, s));
+    ++exp_launches;
+    GPSM_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(ExpandResult), cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    {
+      float ems = 0;
+      GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
+      R.stats.expand_ms += ems;
+    }
+    uint64_t written, consumed_end;
+    if (h_res->cut_row != ~0ULL) {
+      written = h_res->cut_pos;
+      consumed_end = h_res->cut_row;
+    } else {
+      written = std::min<uint64_t>(h_res->total, out_cap);
+      consumed_end = re;
+    }
+    driver_elems += h_res->driver;
+    const uint64_t consumed = consumed_end - rb;
+    alg_bytes += consumed * 4ull * lv + written * 4ull * (lv + 1);
+    if (consumed > 0) A.ratio = std::max(1.0 / 64.0, (double)h_res->total / (double)(re - rb));
+    if (consumed == 0 && written == 0 && !final_level) {
+      set_last_error("a single row produced more rows than a level buffer holds");
+      return GPSM_ERR_BUDGET;
+    }
+    A.next = consumed_end;
+    R.stats.level_rows[lv + 1] += written;
+    if (final_level) {
+      res_used += written;
+      emitted += written;
+      if (emitted >= cap) capped = true;
+      if (!capped && h_res->cut_row != ~0ULL) {
+        // buffer full: drain it and resume from the cut row
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        flush();
+      }
+    } else {
+      L[lv + 1].nrows = written;
+    }
+  }
+  if (emitted >= cap) capped = true;
+  R.stats.expand_launches = exp_launches;
+  R.stats.alg_bytes_join = alg_bytes + driver_elems * 4;
+  R.rows = emitted;
+  R.capped = capped;
+  GPSM_CUDA(cudaEventRecord(ws.ev1, s));
+  if (opt.collect_rows && !opt.keep_on_device) {
+    flush();
+  } else {
+    R.d_rows = res_buf;
+    R.d_rows_count = res_used;
+  }
+  GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4001, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  GPSM_CUDA(cudaEventSynchronize(ws.ev1));
+  GPSM_CUDA(cudaStreamSynchronize(s));
+  if (*reinterpret_cast<uint32_t*>(ws.h_small + 4001) & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {
+    set_last_error("device wait limit or bounds check tripped in the joins");
+    return GPSM_ERR_TIMEOUT;
+  }
+  ws.dirty = false;
+  float ms = 0, ms_f = 0;
+  GPSM_CUDA(cudaEventElapsedTime(&ms, ws.ev0, ws.ev1));
+  GPSM_CUDA(cudaEventElapsedTime(&ms_f, ws.ev0, ws.evm));
+  R.stats.device_ms = ms;
+  R.stats.filter_ms = ms_f;
+  R.stats.join_ms = ms - ms_f;
+  return GPSM_OK;
+}
+
+}  // namespace gpsm

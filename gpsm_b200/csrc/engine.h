@@ -1,0 +1,81 @@
+// Host-side engine: query planning and the per-query device pipeline.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "filter.h"
+#include "internal.h"
+
+namespace gpsm {
+
+DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, const uint32_t* lab, uint32_t n);
+void graph_free(DeviceGraph* g);
+Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles);
+void workspace_free(Workspace* ws);
+
+// The query as the reference's Graph/Match classes see it.
+struct QueryPlan {
+  uint32_t n = 0, m = 0;
+  std::vector<uint32_t> lab;
+  std::vector<std::vector<uint32_t>> in, out;  // file-order directed lists (graph/Graph.cpp:180-185)
+  std::vector<uint32_t> roff, rcol;             // undirected CSR, lists sorted (graph/Graph.cpp:190-226)
+  std::vector<uint32_t> efrom, eto;             // edge ids (match/Match.cu:1738-1754), from < to
+  std::vector<uint32_t> order;                  // filter order (match/Match.cu:339-429)
+  uint32_t deg(uint32_t u) const { return roff[u + 1] - roff[u]; }
+  bool adjacent(uint32_t a, uint32_t b) const;
+  int edge_between(uint32_t a, uint32_t b) const;  // edge id or -1
+};
+
+// Builds the plan; returns GPSM_OK or an error with `err` filled.
+int plan_query(const DeviceGraph& g, uint32_t qn, const uint32_t* qlab, uint32_t qm, const uint32_t* qe,
+               QueryPlan& Q, std::string& err);
+
+// Reference join order from forward candidate-edge sizes
+// (match/Match.cu:1599-1694), restricted to edges with a visited endpoint.
+std::vector<int32_t> plain_order(const QueryPlan& Q, const std::vector<uint64_t>& size_fwd, uint64_t nnz);
+// true when `pos2id` is a permutation in which every vertex after the first
+// has an earlier neighbour.
+bool valid_order(const QueryPlan& Q, const std::vector<int32_t>& pos2id);
+
+enum OrderMode : int { ORDER_PLAIN = 0, ORDER_GIVEN = 1 };
+
+struct MatchOptions {
+  uint64_t cap = ~0ULL;            // embedding cap (rows after which the query stops)
+  int order_mode = ORDER_PLAIN;
+  std::vector<int32_t> given_order;  // pos2id when ORDER_GIVEN
+  uint64_t level_bytes = 256ull << 20;  // per intermediate level buffer
+  uint64_t result_rows = 1ull << 22;    // device result buffer rows before flushing to host
+  bool keep_on_device = false;          // never flush: fail with GPSM_ERR_BUDGET instead
+  bool collect_rows = true;             // false: count only (result rows are discarded)
+  bool filter_only = false;             // stop after the join order (debug entry points)
+};
+
+struct MatchStats {
+  std::vector<uint32_t> cand_count;      // final |C(u)|
+  std::vector<uint64_t> size_fwd, size_rev;  // candidate-edge totals per edge id
+  std::vector<uint64_t> level_rows;      // rows produced at each table width 1..n
+  uint64_t expand_launches = 0;
+  uint64_t filter_launches = 0;
+  double device_ms = 0;
+  double filter_ms = 0, join_ms = 0;
+  uint64_t alg_bytes_join = 0;  // algorithmic bytes of the join phase
+  double expand_ms = 0;         // summed device time of the join launches
+  uint64_t alg_bytes_filter = 0;
+};
+
+struct MatchResult {
+  uint64_t rows = 0;
+  uint32_t cols = 0;
+  bool capped = false;
+  bool empty_filter = false;        // a candidate set ran empty (no embeddings)
+  std::vector<int32_t> id2pos, pos2id;
+  std::vector<uint32_t> host_rows;  // flushed rows (row-major, table column order)
+  uint32_t* d_rows = nullptr;       // rows still on the device (arena memory; valid until the next query)
+  uint64_t d_rows_count = 0;        // rows in d_rows (after host_rows)
+  MatchStats stats;
+};
+
+int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R);
+
+}  // namespace gpsm

@@ -1,0 +1,369 @@
+// Filter-side kernels: candidate initialisation, exploration, refinement,
+// bitmap compaction and candidate-edge collection.
+//
+// Candidate sets live as one bitmap per query vertex (N bits, padded to a
+// multiple of 128 bits) instead of the reference's bool[N] rows: a probe is a
+// 4-byte gather that stays in L2, and compaction reads 16 bytes per 128
+// vertices. Sorted candidate lists and per-word ranks are produced by one
+// single-pass compaction kernel (decoupled look-back, scan.cuh).
+//
+// Semantics follow the reference kernels exactly, because the reference's
+// join order depends on the candidate-edge sizes they produce:
+//   k_mark_range   == check_kernel      (match/Match.cu:431-446)
+//   k_compact      == kernel_collect    (match/Match.cu:463-526)
+//   k_explore      == explore_kernel    (match/Match.cu:528-601)
+//   k_refine       == refine_kernel     (match/Match.cu:761-808)
+//   k_cedge_count  == count_kernel      (match/Match.cu:892-943)
+//   k_cedge_write  == examine_kernel    (match/Match.cu:961-1064)
+#include <cuda_runtime.h>
+
+#include "filter.h"
+#include "scan.cuh"
+
+namespace gpsm {
+
+__global__ void k_mark_range(const uint32_t* __restrict__ ids, uint32_t begin, uint32_t end,
+                             uint32_t* __restrict__ bm) {
+  for (uint32_t i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+    uint32_t x = ids[i];
+    atomicOr(&bm[x >> 5], 1u << (x & 31));
+  }
+}
+
+// One tile = 256 threads x 4 words (uint4) = 1024 words = 32768 vertices.
+constexpr int kCompactBlock = 256;
+constexpr int kCompactWordsPerTile = kCompactBlock * 4;
+
+__global__ void __launch_bounds__(kCompactBlock) k_compact(const uint32_t* __restrict__ bm, uint32_t words,
+                                                          uint32_t* __restrict__ list,
+                                                          uint32_t* __restrict__ rank,
+                                                          uint32_t* __restrict__ count, Lookback lb,
+                                                          uint32_t set_empty_flag) {
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_tile = lb_take_ticket(lb);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t ntiles_c = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
+  if (tile >= ntiles_c) {  // ticket base out of step with the device counter
+    if (threadIdx.x == 0) atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
+    return;
+  }
+  const uint32_t w0 = tile * kCompactWordsPerTile + threadIdx.x * 4;
+  uint4 v = make_uint4(0, 0, 0, 0);
+  if (w0 < words) v = *reinterpret_cast<const uint4*>(bm + w0);  // words is a multiple of 4
+  const uint32_t c0 = __popc(v.x), c1 = __popc(v.y), c2 = __popc(v.z), c3 = __popc(v.w);
+  unsigned long long total;
+  unsigned long long mine = block_exclusive_scan<kCompactBlock>(c0 + c1 + c2 + c3, &total);
+  if (threadIdx.x < 32) {
+    unsigned long long ex = lb_exclusive(lb, tile, total);
+    if (threadIdx.x == 0) s_prefix = ex;
+  }
+  __syncthreads();
+  unsigned long long pos = s_prefix + mine;
+  if (w0 < words) {
+    if (rank) {
+      uint4 r;
+      r.x = (uint32_t)pos;
+      r.y = (uint32_t)(pos + c0);
+      r.z = (uint32_t)(pos + c0 + c1);
+      r.w = (uint32_t)(pos + c0 + c1 + c2);
+      *reinterpret_cast<uint4*>(rank + w0) = r;
+    }
+    uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      uint32_t x = wv[k];
+      while (x) {
+        int b = __ffs(x) - 1;
+        x &= x - 1;
+        list[pos++] = (w0 + k) * 32 + b;
+      }
+    }
+  }
+  const uint32_t ntiles = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
+  if (tile == ntiles - 1 && threadIdx.x == 0) {
+    unsigned long long c = s_prefix + total;
+    *count = (uint32_t)c;
+    if (set_empty_flag && c == 0) atomicOr(lb.flags, (uint32_t)DF_EMPTY);
+  }
+}
+
+// Warp per candidate mu of u. For each target v (label, degree) in order:
+// every neighbour mv of mu with that label and degree >= deg(v) enters C(v);
+// if none does, mu leaves C(u) and later targets are skipped.
+__global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __restrict__ list,
+                                                 const uint32_t* __restrict__ count, uint32_t u,
+                                                 const uint32_t* __restrict__ tgt, uint32_t ntgt,
+                                                 uint32_t* __restrict__ bm, uint32_t words,
+                                                 const uint32_t* __restrict__ flags) {
+  extern __shared__ uint32_t s_tgt[];  // 3 * ntgt: v, label, degree
+  for (uint32_t i = threadIdx.x; i < 3 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
+  __syncthreads();
+  if (*flags & DF_EMPTY) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = *count;
+  uint32_t* bmu = bm + (size_t)u * words;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
+    const uint32_t mu = list[w];
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    for (uint32_t t = 0; t < ntgt; ++t) {
+      const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
+      uint32_t* bmv = bm + (size_t)v * words;
+      bool any = false;
+      for (uint32_t j = b + lane; j < e; j += 32) {
+        const uint32_t mv = g.col[j];
+        const uint2 ld = g.labdeg[mv];
+        if (ld.x == lv && ld.y >= dv) {
+          atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
+          any = true;
+        }
+      }
+      if (!__any_sync(0xffffffffu, any)) {
+        if (lane == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        break;
+      }
+    }
+  }
+}
+
+// Warp per candidate mu of u: mu stays only if every target v has a
+// candidate among mu's neighbours.
+__global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __restrict__ list,
+                                                const uint32_t* __restrict__ count, uint32_t u,
+                                                const uint32_t* __restrict__ tgt, uint32_t ntgt,
+                                                uint32_t* __restrict__ bm, uint32_t words,
+                                                const uint32_t* __restrict__ flags) {
+  extern __shared__ uint32_t s_tgt[];
+  for (uint32_t i = threadIdx.x; i < ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
+  __syncthreads();
+  if (*flags & DF_EMPTY) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t n = *count;
+  uint32_t* bmu = bm + (size_t)u * words;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
+    const uint32_t mu = list[w];
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    for (uint32_t t = 0; t < ntgt; ++t) {
+      const uint32_t* bmv = bm + (size_t)s_tgt[t] * words;
+      bool found = false;
+      for (uint32_t j0 = b; j0 < e; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        bool hit = false;
+        if (j < e) {
+          const uint32_t mv = g.col[j];
+          hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+        }
+        if (__any_sync(0xffffffffu, hit)) {
+          found = true;
+          break;
+        }
+      }
+      if (!found) {
+        if (lane == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        break;
+      }
+    }
+  }
+}
+
+// Work item i belongs to edge-direction d with item_base[d] <= i < item_base[d+1].
+__device__ __forceinline__ uint32_t find_dir(const unsigned long long* __restrict__ s_base, uint32_t ndir,
+                                             unsigned long long i) {
+  uint32_t lo = 0, hi = ndir;  // invariant: s_base[lo] <= i < s_base[hi]
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (s_base[mid] <= i) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Per (edge direction u->v, mu in C(u)): |N(mu) ∩ C(v)|.
+__global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir* __restrict__ dirs,
+                                                     uint32_t ndir, const unsigned long long* __restrict__ s_base,
+                                                     const uint32_t* __restrict__ bm, uint32_t words,
+                                                     uint32_t* __restrict__ cnt) {
+  const unsigned long long items = s_base[ndir];
+  const uint32_t lane = threadIdx.x & 31;
+  const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += warps) {
+    const uint32_t d = find_dir(s_base, ndir, w);
+    const CedgeDir cd = dirs[d];
+    const uint32_t mu = cd.ids[w - cd.item_base];
+    const uint32_t* bmv = bm + (size_t)cd.v * words;
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    uint32_t c = 0;
+    for (uint32_t j = b + lane; j < e; j += 32) {
+      const uint32_t mv = g.col[j];
+      c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[w] = c;
+  }
+}
+
+// Writes N(mu) ∩ C(v) in adjacency (ascending) order at goff[item].
+__global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir* __restrict__ dirs,
+                                                     uint32_t ndir, const unsigned long long* __restrict__ s_base,
+                                                     const uint32_t* __restrict__ bm, uint32_t words,
+                                                     const unsigned long long* __restrict__ goff,
+                                                     uint32_t* __restrict__ nbrs) {
+  const unsigned long long items = s_base[ndir];
+  const uint32_t lane = threadIdx.x & 31;
+  const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += warps) {
+    const uint32_t d = find_dir(s_base, ndir, w);
+    const CedgeDir cd = dirs[d];
+    const uint32_t mu = cd.ids[w - cd.item_base];
+    const uint32_t* bmv = bm + (size_t)cd.v * words;
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    unsigned long long pos = goff[w];
+    for (uint32_t j0 = b; j0 < e; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      uint32_t mv = 0;
+      bool hit = false;
+      if (j < e) {
+        mv = g.col[j];
+        hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) nbrs[pos + __popc(bal & ((1u << lane) - 1))] = mv;
+      pos += __popc(bal);
+    }
+  }
+}
+
+// Exclusive scan of n uint32 counts into n+1 uint64 offsets (out[n] = total).
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 8;
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_u32(const uint32_t* __restrict__ in, unsigned long long n,
+                                                        unsigned long long* __restrict__ out, Lookback lb) {
+  __shared__ uint32_t s_tile;
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_tile = lb_take_ticket(lb);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  {
+    const unsigned long long per = (unsigned long long)kScanBlock * kScanItems;
+    const unsigned long long nt = (n + per - 1) / per;
+    if ((unsigned long long)tile >= (nt ? nt : 1)) {
+      if (threadIdx.x == 0) atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
+      return;
+    }
+  }
+  const unsigned long long i0 = ((unsigned long long)tile * kScanBlock + threadIdx.x) * kScanItems;
+  uint32_t v[kScanItems];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (i0 + k < n) ? in[i0 + k] : 0;
+    s += v[k];
+  }
+  unsigned long long total;
+  unsigned long long mine = block_exclusive_scan<kScanBlock>(s, &total);
+  if (threadIdx.x < 32) {
+    unsigned long long ex = lb_exclusive(lb, tile, total);
+    if (threadIdx.x == 0) s_prefix = ex;
+  }
+  __syncthreads();
+  unsigned long long pos = s_prefix + mine;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (i0 + k < n) out[i0 + k] = pos;
+    pos += v[k];
+  }
+  const unsigned long long per_tile = (unsigned long long)kScanBlock * kScanItems;
+  const unsigned long long ntiles = (n + per_tile - 1) / per_tile;
+  if (threadIdx.x == 0 && (unsigned long long)tile == (ntiles ? ntiles - 1 : 0)) out[n] = s_prefix + total;
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static Lookback make_lb(Workspace& ws, uint32_t tiles) {
+  Lookback lb;
+  lb.ticket = ws.scan.d_ticket;
+  lb.status = ws.scan.d_status;
+  unsigned long long base;
+  uint32_t ep;
+  if (tiles > ws.scan.max_tiles) {
+    set_last_error("scan: too many tiles");
+    throw CudaError{cudaErrorInvalidValue, "scan tiles"};
+  }
+  ws.scan.next_launch(tiles, &base, &ep);
+  lb.base = base;
+  lb.epoch = ep;
+  lb.flags = ws.d_flags;
+  return lb;
+}
+
+static uint32_t grid_for(uint64_t warps_needed, uint32_t cap_blocks) {
+  uint64_t blocks = (warps_needed + 7) / 8;
+  if (blocks < 1) blocks = 1;
+  if (blocks > cap_blocks) blocks = cap_blocks;
+  return (uint32_t)blocks;
+}
+
+void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint32_t end, uint32_t* bm) {
+  if (end <= begin) return;
+  uint32_t blocks = (uint32_t)std::min<uint64_t>((end - begin + 255) / 256, 148 * 8);
+  k_mark_range<<<blocks, 256, 0, ws.stream>>>(g.lab_vtx, begin, end, bm);
+  GPSM_LAUNCHED();
+}
+
+void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t* list, uint32_t* rank,
+                    uint32_t* count, bool set_empty_flag) {
+  uint32_t tiles = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
+  Lookback lb = make_lb(ws, tiles);
+  k_compact<<<tiles, kCompactBlock, 0, ws.stream>>>(bm, words, list, rank, count, lb, set_empty_flag ? 1u : 0u);
+  GPSM_LAUNCHED();
+}
+
+void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
+                    uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
+  if (ntgt == 0 || max_count == 0) return;
+  uint32_t blocks = grid_for(max_count, 148 * 16);
+  k_explore<<<blocks, 256, 3 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm,
+                                                                    g.words, ws.d_flags);
+  GPSM_LAUNCHED();
+}
+
+void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
+                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
+  if (ntgt == 0 || max_count == 0) return;
+  uint32_t blocks = grid_for(max_count, 148 * 16);
+  k_refine<<<blocks, 256, ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
+                                                               ws.d_flags);
+  GPSM_LAUNCHED();
+}
+
+void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
+                        const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt) {
+  if (items == 0) return;
+  uint32_t blocks = grid_for(items, 148 * 16);
+  k_cedge_count<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, cnt);
+  GPSM_LAUNCHED();
+}
+
+void launch_cedge_write(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
+                        const unsigned long long* d_base, uint64_t items, const uint32_t* bm,
+                        const unsigned long long* goff, uint32_t* nbrs) {
+  if (items == 0) return;
+  uint32_t blocks = grid_for(items, 148 * 16);
+  k_cedge_write<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, goff, nbrs);
+  GPSM_LAUNCHED();
+}
+
+void launch_scan_u32(Workspace& ws, const uint32_t* in, uint64_t n, unsigned long long* out) {
+  const uint64_t per_tile = (uint64_t)kScanBlock * kScanItems;
+  uint32_t tiles = (uint32_t)std::max<uint64_t>(1, (n + per_tile - 1) / per_tile);
+  Lookback lb = make_lb(ws, tiles);
+  k_scan_u32<<<tiles, kScanBlock, 0, ws.stream>>>(in, n, out, lb);
+  GPSM_LAUNCHED();
+}
+
+}  // namespace gpsm

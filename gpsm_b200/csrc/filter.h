@@ -1,0 +1,71 @@
+// Kernel launchers shared by the engine (device code in filter.cu / join.cu).
+#pragma once
+#include "internal.h"
+
+namespace gpsm {
+
+// Plain device pointers of a DeviceGraph, passed by value to kernels.
+struct GraphView {
+  const uint32_t* __restrict__ off;
+  const uint32_t* __restrict__ col;
+  const uint2* __restrict__ labdeg;
+  uint32_t n;
+};
+
+inline GraphView view(const DeviceGraph& g) { return GraphView{g.off, g.col, g.labdeg, g.n}; }
+
+// One direction u->v of a query edge for candidate-edge collection.
+struct CedgeDir {
+  const uint32_t* ids;           // final sorted candidate list of u
+  uint32_t n;                    // |C(u)|
+  uint32_t v;                    // target query vertex (its bitmap is probed)
+  unsigned long long item_base;  // first work item (index into counts/offsets)
+};
+
+void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint32_t end, uint32_t* bm);
+void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t* list, uint32_t* rank,
+                    uint32_t* count, bool set_empty_flag);
+void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
+                    uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
+void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
+                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
+// d_base[ndir+1]: first work item of each direction, d_base[ndir] = items
+void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
+                        const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt);
+void launch_cedge_write(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
+                        const unsigned long long* d_base, uint64_t items, const uint32_t* bm,
+                        const unsigned long long* goff, uint32_t* nbrs);
+void launch_scan_u32(Workspace& ws, const uint32_t* in, uint64_t n, unsigned long long* out);
+void launch_gather_u64(Workspace& ws, const unsigned long long* src, const unsigned long long* idx, uint32_t n,
+                       unsigned long long* dst);
+
+// ---- joins ---------------------------------------------------------------
+// An already-placed query neighbour w of the vertex being added.
+struct BackNbr {
+  uint32_t col;                         // column of w in the input table
+  uint32_t pad;
+  const uint32_t* bm;                   // final C(w) bitmap
+  const uint32_t* rank;                 // per-word ranks of C(w)
+  const unsigned long long* off;        // candidate-edge offsets of w->v, by rank of mu in C(w)
+  const uint32_t* nbrs;                 // candidate-edge neighbour array
+};
+
+constexpr uint32_t kMaxBack = 128;  // query vertices are < 128 here; checked on the host
+
+struct ExpandResult {  // device-side result words of one expand launch
+  unsigned long long total;     // sum of row output counts over all input rows processed
+  unsigned long long cut_pos;   // output position of the first row not written (~0 = none)
+  unsigned long long cut_row;   // first input row not written (~0 = none)
+  unsigned long long driver;    // sum over rows of the driving list length (pass 1)
+};
+
+// Expands input rows [row_begin, row_end) (in_cols columns, row-major) by one
+// query vertex whose placed neighbours are `back[0..nb)`. Outputs go to
+// `out` (in_cols+1 columns) up to out_cap rows; when `partial` is set the
+// last row may be cut inside (embedding cap). res must be initialised.
+// nbrs_total bounds every candidate-edge range (a failed check raises DF_BOUNDS).
+void launch_expand(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
+                   const BackNbr* d_back, uint32_t nb, uint32_t* out, uint64_t out_cap, bool partial,
+                   ExpandResult* d_res, uint64_t nbrs_total);
+
+}  // namespace gpsm

@@ -1,0 +1,121 @@
+// Internal structures of the engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "gpsm.h"
+
+namespace gpsm {
+
+// ---------------------------------------------------------------------------
+// error plumbing: every CUDA call is checked; failures become GPSM_ERR_CUDA
+// (the reference exits the process instead, match/Match.h:53-65)
+// ---------------------------------------------------------------------------
+struct CudaError {
+  cudaError_t err;
+  const char* what;
+};
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+#define GPSM_CUDA(call)                                                                    \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      ::gpsm::set_last_error(std::string(#call) + ": " + cudaGetErrorString(e_) + " at " + \
+                             __FILE__ + ":" + std::to_string(__LINE__));                   \
+      throw ::gpsm::CudaError{e_, #call};                                                  \
+    }                                                                                      \
+  } while (0)
+
+#define GPSM_LAUNCHED() GPSM_CUDA(cudaGetLastError())
+
+// device-side error flags (bitwise OR into Workspace::d_flags[0])
+enum DeviceFlag : uint32_t {
+  DF_EMPTY = 1u << 0,       // a candidate set collected empty (no embedding exists)
+  DF_SCAN_TIMEOUT = 1u << 1,  // a decoupled look-back wait hit its iteration limit
+  DF_BOUNDS = 1u << 2,      // an index check failed (result invalid)
+  DF_OVERFLOW = 1u << 3,    // a 32-bit count overflowed
+};
+
+// ---------------------------------------------------------------------------
+// device-resident data graph (uploaded once, reused by every query)
+// ---------------------------------------------------------------------------
+struct DeviceGraph {
+  int device = 0;
+  uint32_t n = 0;
+  uint64_t nnz = 0;           // offsets[n] = 2 * undirected edges
+  uint32_t* off = nullptr;    // [n+1]
+  uint32_t* col = nullptr;    // [nnz], each list sorted ascending
+  uint32_t* lab = nullptr;    // [n]
+  uint2* labdeg = nullptr;    // [n] (label, degree): one 8-byte gather per neighbour
+  uint32_t* lab_vtx = nullptr;  // [n] vertices grouped by label, degree descending
+  // host-side label index (labels sorted ascending)
+  std::vector<uint32_t> h_labels;   // distinct labels
+  std::vector<uint32_t> h_lab_ptr;  // [L+1] offsets into lab_vtx
+  std::vector<uint32_t> h_lab_deg;  // [n] degrees in lab_vtx order (for cut-offs)
+  uint32_t words = 0;               // bitmap words per candidate set (padded to 4)
+  uint32_t max_degree = 0;
+  // label frequency as the reference computes it (Graph::inverse_num)
+  uint64_t label_count(uint32_t label) const;
+  // [begin, end) of lab_vtx for vertices with `label` and degree >= d
+  void label_range(uint32_t label, uint32_t d, uint32_t* begin, uint32_t* end) const;
+};
+
+// ---------------------------------------------------------------------------
+// decoupled look-back scan state: tiles take tickets in launch order from a
+// monotone 64-bit counter whose per-launch base the host tracks, and publish
+// (epoch, flag, value) words; no memset between scans is needed.
+// ---------------------------------------------------------------------------
+struct ScanState {
+  unsigned long long* d_ticket = nullptr;  // monotone ticket counter
+  unsigned long long* d_status = nullptr;  // [max_tiles] status words
+  uint32_t max_tiles = 0;
+  unsigned long long ticket_base = 0;  // host copy of the counter value before the next launch
+  uint32_t epoch = 0;        // 20-bit epoch of the next launch
+  // reserve `tiles` tickets for one launch; returns (base, epoch)
+  void next_launch(uint32_t tiles, unsigned long long* base, uint32_t* ep) {
+    *base = ticket_base;
+    ticket_base += tiles;
+    epoch = (epoch + 1) & 0xFFFFF;
+    if (epoch == 0) epoch = 1;
+    *ep = epoch;
+  }
+};
+
+// bump allocator over one device allocation; reset per query
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0;
+  size_t used = 0;
+  size_t high_water = 0;
+  void* alloc(size_t bytes, size_t align = 256) {
+    size_t p = (used + align - 1) & ~(align - 1);
+    if (p + bytes > size) return nullptr;
+    used = p + bytes;
+    if (used > high_water) high_water = used;
+    return base + p;
+  }
+  void reset() { used = 0; }
+};
+
+struct Workspace {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  ScanState scan;
+  uint32_t* d_flags = nullptr;      // [16] device flags and small counters
+  unsigned long long* d_small = nullptr;  // [64] device scratch for results of scans
+  unsigned long long* h_small = nullptr;  // pinned mirror
+  cudaEvent_t ev0 = nullptr, evm = nullptr, ev1 = nullptr;
+  cudaEvent_t eve0 = nullptr, eve1 = nullptr;  // around each join launch
+  cudaEvent_t evb0 = nullptr, evb1 = nullptr;  // around a batch
+  bool dirty = false;  // a query stopped part-way; resynchronise scan tickets
+};
+
+}  // namespace gpsm

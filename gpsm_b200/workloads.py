@@ -1,0 +1,192 @@
+"""Seeded synthetic data graphs and query sets for the five workload shapes.
+
+No public dataset is named for this path and the reference's benchmark
+datasets (script/run.sh: delaunay_n13, enron, gowalla, road_central) are not
+available, so every workload is generated from a seed:
+
+  small_er     ER G(10,000, 40,000), labels U{1..8}; 10 induced random-walk
+               queries of 6 vertices
+  rmat20       R-MAT(.57,.19,.19,.05) on 2^20 vertices, 16 Mi undirected edges,
+               labels Zipf(1.0) over 1..32; 100 induced random-walk queries of
+               12 vertices with average degree >= 2.5
+  rmat20_mix   the rmat20 graph; 1,000 queries of 4..32 vertices, half tree
+               (n-1 edges), half dense (extra induced edges kept with p=0.3)
+  rmat22       R-MAT on 2^22 vertices, 64 Mi edges, Zipf(1.1) over 1..64;
+               4,096 queries of 4..64 vertices (tree/dense mix)
+  rmat24       R-MAT on 2^24 vertices, 256 Mi edges, Zipf(1.0) over 1..128;
+               queries of 4..99 vertices, geometric with mean 16
+All generation runs in libgpsm.so (gen.cpp); this module only sequences it.
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+MODE_INDUCED, MODE_TREE, MODE_DENSE = 0, 1, 2
+
+
+@dataclass
+class Graph:
+    """Undirected data graph: CSR with sorted lists plus the edge list."""
+    n: int
+    offsets: np.ndarray  # uint32 [n+1]
+    cols: np.ndarray  # uint32 [2m]
+    labels: np.ndarray  # uint32 [n], 1-based
+    edges: np.ndarray  # uint32 [m, 2], each undirected edge once
+    name: str = ""
+
+    @property
+    def m(self):
+        return int(self.edges.shape[0])
+
+
+@dataclass
+class Query:
+    labels: np.ndarray  # uint32 [qn]
+    edges: np.ndarray  # uint32 [qm, 2] (from, to) in file order
+    data_ids: np.ndarray = None  # the walked data vertices (one known match)
+    seed: int = 0
+
+    @property
+    def n(self):
+        return int(self.labels.shape[0])
+
+    @property
+    def m(self):
+        return int(self.edges.shape[0])
+
+
+@dataclass
+class Workload:
+    name: str
+    graph: Graph
+    queries: list = field(default_factory=list)
+
+
+def _mix(a, b):
+    x = (a * 0x9E3779B97F4A7C15 + b + 0x632BE59BD9B4E019) & 0xFFFFFFFFFFFFFFFF
+    x ^= x >> 30
+    x = (x * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    x ^= x >> 27
+    x = (x * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x ^ (x >> 31)
+
+
+def graph_from_edges(n, edges, labels, name=""):
+    lib = _lib.load()
+    edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
+    m = edges.shape[0]
+    off = np.zeros(n + 1, dtype=np.uint32)
+    cols = np.zeros(max(2 * m, 1), dtype=np.uint32)
+    _lib.check(lib.gpsm_csr_from_edges(n, m, _lib.ptr(edges), _lib.ptr(off), _lib.ptr(cols)), "csr")
+    return Graph(n, off, cols[: 2 * m], _lib.u32a(labels), edges, name)
+
+
+def er_graph(n, m, num_labels, seed, zipf_s=0.0, name="er"):
+    lib = _lib.load()
+    edges = np.zeros((m, 2), dtype=np.uint32)
+    _lib.check(lib.gpsm_gen_er(n, m, seed, _lib.ptr(edges)), "gen_er")
+    labels = np.zeros(n, dtype=np.uint32)
+    _lib.check(lib.gpsm_gen_labels(n, num_labels, zipf_s, _mix(seed, 7), _lib.ptr(labels)), "labels")
+    return graph_from_edges(n, edges, labels, name)
+
+
+def rmat_graph(scale, m, num_labels, zipf_s, seed, a=0.57, b=0.19, c=0.19, name="rmat"):
+    lib = _lib.load()
+    edges = np.zeros((m, 2), dtype=np.uint32)
+    _lib.check(lib.gpsm_gen_rmat(scale, m, a, b, c, seed, _lib.ptr(edges)), "gen_rmat")
+    n = 1 << scale
+    labels = np.zeros(n, dtype=np.uint32)
+    _lib.check(lib.gpsm_gen_labels(n, num_labels, zipf_s, _mix(seed, 7), _lib.ptr(labels)), "labels")
+    return graph_from_edges(n, edges, labels, name)
+
+
+def random_walk_query(g, qn, seed, mode=MODE_INDUCED, p_extra=0.0, min_avg_degree=0.0):
+    lib = _lib.load()
+    ql = np.zeros(qn, dtype=np.uint32)
+    qe = np.zeros(max(qn * (qn - 1), 2), dtype=np.uint32)
+    ids = np.zeros(qn, dtype=np.uint32)
+    r = lib.gpsm_gen_query(g.n, _lib.ptr(g.offsets), _lib.ptr(g.cols), _lib.ptr(g.labels), qn, mode,
+                           p_extra, min_avg_degree, seed, _lib.ptr(ql), _lib.ptr(qe), _lib.ptr(ids))
+    _lib.check(r, "gen_query")
+    return Query(ql, qe[: 2 * r].reshape(-1, 2).copy(), ids, seed)
+
+
+def _size_stream(rng, kind, count, lo, hi, mean=None):
+    if kind == "fixed":
+        return [lo] * count
+    if kind == "uniform":
+        return [int(x) for x in rng.integers(lo, hi + 1, size=count)]
+    if kind == "geometric":  # mean `mean`, clipped to [lo, hi]
+        p = 1.0 / mean
+        return [int(min(hi, max(lo, x))) for x in rng.geometric(p, size=count)]
+    raise ValueError(kind)
+
+
+def query_set(g, count, seed, sizes=("fixed", 6, 6), mix="induced", p_extra=0.3,
+              min_avg_degree=0.0, mean=None):
+    """count random-walk queries; mix is 'induced', 'tree', 'dense' or 'tree_dense' (50/50)."""
+    rng = np.random.default_rng(_mix(seed, 0x512E))
+    qsizes = _size_stream(rng, sizes[0], count, sizes[1], sizes[2], mean)
+    out = []
+    for k in range(count):
+        qs = _mix(seed, 1000 + k)
+        if mix == "induced":
+            mode = MODE_INDUCED
+        elif mix == "tree":
+            mode = MODE_TREE
+        elif mix == "dense":
+            mode = MODE_DENSE
+        else:
+            mode = MODE_TREE if k % 2 == 0 else MODE_DENSE
+        out.append(random_walk_query(g, qsizes[k], qs, mode, p_extra, min_avg_degree))
+    return out
+
+
+_GRAPH_CACHE = {}
+
+
+def graph_for(name, seed=0):
+    key = (name, seed)
+    if key in _GRAPH_CACHE:
+        return _GRAPH_CACHE[key]
+    if name == "small_er":
+        g = er_graph(10_000, 40_000, 8, _mix(seed, 1), name=name)
+    elif name == "rmat20":
+        g = rmat_graph(20, 16 << 20, 32, 1.0, _mix(seed, 2), name=name)
+    elif name == "rmat22":
+        g = rmat_graph(22, 64 << 20, 64, 1.1, _mix(seed, 4), name=name)
+    elif name == "rmat24":
+        g = rmat_graph(24, 256 << 20, 128, 1.0, _mix(seed, 5), name=name)
+    else:
+        raise ValueError(name)
+    _GRAPH_CACHE[key] = g
+    return g
+
+
+def workload(name, seed=0, count=None):
+    """The named workload: graph plus its query set (count overrides the size)."""
+    if name == "small_er":
+        g = graph_for("small_er", seed)
+        qs = query_set(g, count or 10, _mix(seed, 11), ("fixed", 6, 6), "induced")
+    elif name == "rmat20":
+        g = graph_for("rmat20", seed)
+        qs = query_set(g, count or 100, _mix(seed, 12), ("fixed", 12, 12), "induced",
+                       min_avg_degree=2.5)
+    elif name == "rmat20_mix":
+        g = graph_for("rmat20", seed)
+        qs = query_set(g, count or 1000, _mix(seed, 13), ("uniform", 4, 32), "tree_dense", 0.3)
+    elif name == "rmat20_train":
+        g = graph_for("rmat20", seed)
+        qs = query_set(g, count or 5000, _mix(seed, 14), ("uniform", 4, 32), "tree_dense", 0.3)
+    elif name == "rmat22":
+        g = graph_for("rmat22", seed)
+        qs = query_set(g, count or 4096, _mix(seed, 15), ("uniform", 4, 64), "tree_dense", 0.3)
+    elif name == "rmat24":
+        g = graph_for("rmat24", seed)
+        qs = query_set(g, count or 2000, _mix(seed, 16), ("geometric", 4, 99), "tree_dense", 0.3,
+                       mean=16)
+    else:
+        raise ValueError(name)
+    return Workload(name, g, qs)

@@ -1,0 +1,173 @@
+/* gpsm.h - C ABI of the B200 subgraph-matching engine (libgpsm.so).
+ *
+ * Plain pointers and sizes only. Every entry point returns an int status
+ * (GPSM_OK or a negative GPSM_ERR_*); the reference instead calls exit(1) on
+ * any CUDA error (match/Match.h:53-65).
+ *
+ * Conventions shared with the reference's file format and classes:
+ *   - vertex ids are 0-based, labels are 1-based unsigned (README.md);
+ *   - a data graph is an undirected CSR: offsets[n+1], cols[offsets[n]] with
+ *     every adjacency list sorted ascending (graph/Graph.cpp:190-226);
+ *   - a query is (qn labels, qm edges as (from, to) pairs in file order),
+ *     exactly what io/IO.cpp:87-142 reads from `v`/`e` lines.
+ * Embeddings are non-induced, injective, undirected and edge-unlabelled.
+ */
+#ifndef GPSM_H
+#define GPSM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define GPSM_OK 0
+#define GPSM_ERR_INVALID -1   /* bad argument or malformed graph */
+#define GPSM_ERR_CUDA -2      /* a CUDA runtime call failed */
+#define GPSM_ERR_NOMEM -3     /* device or host allocation failed */
+#define GPSM_ERR_NOT_FOUND -4 /* generator could not find a query */
+#define GPSM_ERR_BUDGET -5    /* request exceeds the memory budget */
+#define GPSM_ERR_TIMEOUT -6   /* a bounded device-side wait gave up */
+#define GPSM_ERR_NODEV -7     /* no CUDA device */
+#define GPSM_ERR_STATE -8     /* call order violated (e.g. no gpsm_init) */
+
+/* ---- synthetic workloads (host) --------------------------------------- */
+/* Erdos-Renyi G(n, m): m unique undirected edges (u < v), no self loops.
+ * edges: 2*m uint32. */
+int gpsm_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t* edges);
+/* R-MAT over 2^scale vertices with quadrant probabilities a, b, c
+ * (d = 1-a-b-c): exactly m unique undirected edges, no self loops, vertex ids
+ * randomly permuted. edges: 2*m uint32, each pair (min, max). */
+int gpsm_gen_rmat(int scale, uint64_t m, double a, double b, double c, uint64_t seed,
+                  uint32_t* edges);
+/* i.i.d. vertex labels in 1..num_labels with P(k) ~ k^-zipf_s (0 = uniform). */
+int gpsm_gen_labels(uint32_t n, uint32_t num_labels, double zipf_s, uint64_t seed,
+                    uint32_t* labels);
+/* Undirected CSR from m undirected edges; each list sorted ascending.
+ * offsets: n+1, cols: 2*m. Replaces Graph::transformToCSR (graph/Graph.cpp:190-226). */
+int gpsm_csr_from_edges(uint32_t n, uint64_t m, const uint32_t* edges, uint32_t* offsets,
+                        uint32_t* cols);
+/* Random-walk query of qn vertices (mode 0 induced, 1 tree, 2 dense with
+ * p_extra). q_labels: qn; q_edges: qn*(qn-1) uint32; q_data_ids: qn or NULL.
+ * Returns the number of query edges (>= 0) or a negative status. */
+int64_t gpsm_gen_query(uint32_t n, const uint32_t* offsets, const uint32_t* cols,
+                       const uint32_t* labels, uint32_t qn, int mode, double p_extra,
+                       double min_avg_degree, uint64_t seed, uint32_t* q_labels,
+                       uint32_t* q_edges, uint32_t* q_data_ids);
+
+/* ---- engine: device, data graph, matching ------------------------------ */
+typedef struct gpsm_graph_s* gpsm_graph_t;   /* device-resident data graph */
+typedef struct gpsm_engine_s* gpsm_engine_t; /* stream + workspace on one device */
+
+/* Text of the last error on the calling thread. */
+const char* gpsm_last_error(void);
+
+/* Selects device `dev` and creates the default engine (workspace arena of
+ * arena_bytes; 0 = min(16 GiB, 60% of free memory), or GPSM_ARENA_GB).
+ * Replaces Match::initGPU (match/Match.cu:15-70), which exits when no device
+ * exists and reserves a 4 GB device heap for kernel-side new/delete. */
+int gpsm_init(int dev);
+int gpsm_init_ex(int dev, uint64_t arena_bytes);
+int gpsm_shutdown(void);
+
+/* Additional engines (one stream and arena each) for concurrent callers. */
+int gpsm_engine_create(int dev, uint64_t arena_bytes, gpsm_engine_t* out);
+int gpsm_engine_destroy(gpsm_engine_t e);
+
+/* Uploads an undirected CSR (offsets[n+1], cols[offsets[n]], labels[n]) once;
+ * every later query reuses it. Replaces Match::copyGraphToGPU
+ * (match/Match.cu:128-143), which re-uploads the graph for every query. */
+int gpsm_graph_upload(const uint32_t* offsets, const uint32_t* cols, const uint32_t* labels,
+                      uint32_t n, gpsm_graph_t* out);
+int gpsm_graph_free(gpsm_graph_t g);
+int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_degree);
+
+#define GPSM_ORDER_PLAIN 0 /* the reference's join order (match/Match.cu:1599-1694) */
+#define GPSM_ORDER_GIVEN 1 /* opts.order gives the table columns (pos -> query vertex) */
+
+#define GPSM_F_COUNT_ONLY 1u      /* do not return rows (count and statistics only) */
+#define GPSM_F_KEEP_ON_DEVICE 2u  /* rows stay in device memory; never spill to host */
+
+typedef struct gpsm_match_opts {
+  uint64_t cap;          /* embedding cap: stop after the first `cap` rows; 0 = none */
+  int32_t order_mode;    /* GPSM_ORDER_* */
+  int32_t pad;
+  const int32_t* order;  /* pos2id[qn] for GPSM_ORDER_GIVEN */
+  uint64_t level_bytes;  /* bytes per intermediate join level; 0 = 256 MiB */
+  uint64_t result_rows;  /* device result buffer rows; 0 = 4 Mi */
+  uint32_t flags;        /* GPSM_F_* */
+  uint32_t pad2;
+} gpsm_match_opts;
+
+typedef struct gpsm_match_info {
+  uint64_t rows;             /* embeddings returned (== cap when capped) */
+  uint32_t cols;             /* query vertices */
+  int32_t capped;            /* 1 when the cap stopped the query */
+  int32_t empty_filter;      /* 1 when a candidate set ran empty */
+  int32_t pad;
+  double device_ms;          /* device time of the whole query */
+  double filter_ms;          /* filter + candidate edges */
+  double join_ms;            /* joins */
+  uint64_t expand_launches;
+  uint64_t filter_launches;
+  uint64_t alg_bytes_join;   /* algorithmic bytes of the joins (roofline numerator) */
+  double expand_ms;          /* summed device time of the join launches */
+} gpsm_match_info;
+
+typedef struct gpsm_batch_info {
+  double device_ms;          /* engine-stream events: first query start to last query end */
+  double expand_ms;          /* summed device time of the join launches */
+  double filter_ms;          /* summed filter + candidate-edge time */
+  uint64_t rows;             /* embeddings over the batch */
+  uint64_t launches;         /* kernels launched by the batch */
+  uint64_t expand_launches;
+  uint64_t alg_bytes_join;
+} gpsm_batch_info;
+
+/* Matches one query. Replaces Match::match (match/Match.cu:1710-1966).
+ * Rows are row-major with qn columns in table-column order; column p holds
+ * query vertex pos2id[p], so query vertex j of row r is
+ * rows[r*qn + id_map[j]] (the reference's id_map convention, run.cpp:76-84).
+ * *out_rows is malloc'd (free with gpsm_free); NULL out_rows = count only.
+ * id_map and pos2id (qn entries each) may be NULL. */
+int gpsm_match_ex(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
+                  const uint32_t* q_edges, const gpsm_match_opts* opts, uint32_t** out_rows,
+                  int32_t* id_map, int32_t* pos2id, gpsm_match_info* info);
+int gpsm_engine_match(gpsm_engine_t e, gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels,
+                      uint32_t qm, const uint32_t* q_edges, const gpsm_match_opts* opts,
+                      uint32_t** out_rows, int32_t* id_map, int32_t* pos2id, gpsm_match_info* info);
+/* Shorthand: plain order, optional cap (0 = none). */
+int gpsm_match(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
+               const uint32_t* q_edges, uint64_t cap, uint32_t** out_rows, uint64_t* out_nrows,
+               uint32_t* out_ncols, int32_t* id_map);
+void gpsm_free(void* p);
+
+/* Matches nq queries back to back (query k: labels q_labels[q_voff[k]..],
+ * edges q_edges[2*q_eoff[k]..]); rows are produced in device memory and
+ * overwritten by the next query. orders: concatenated pos2id per query when
+ * opts->order_mode is GPSM_ORDER_GIVEN. counts, capped, query_ms: nq each or
+ * NULL. A throughput entry point with no counterpart in the reference, whose
+ * run.cpp loops Match::match per query (main/run.cpp:60-97). */
+int gpsm_match_batch(gpsm_engine_t e, gpsm_graph_t g, uint32_t nq, const uint32_t* q_voff,
+                     const uint32_t* q_labels, const uint64_t* q_eoff, const uint32_t* q_edges,
+                     const gpsm_match_opts* opts, const int32_t* orders, uint64_t* counts,
+                     int32_t* capped, double* query_ms, gpsm_batch_info* info);
+/* Writes `bytes` of device memory on the engine's stream (an L2 flush). */
+int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
+
+/* Filter-stage results for comparison with the reference restatement:
+ * final |C(u)|, candidate-edge totals per edge id (forward = from->to with
+ * from < to, reverse = to->from), the filter (BFS) order, the plain join
+ * order and optionally every candidate set as qn*N bytes (0/1).
+ * Returns 1 (not an error) when a candidate set ran empty. */
+int gpsm_debug_filter(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
+                      const uint32_t* q_edges, uint32_t* cand_count, uint64_t* size_fwd,
+                      uint64_t* size_rev, uint32_t* filter_order, int32_t* plain_pos2id,
+                      uint8_t* cand_bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPSM_H */

@@ -1,0 +1,185 @@
+"""ORACLE - test infrastructure only.
+
+ctypes wrapper of liboracle.so (oracle.cpp): the independent backtracking
+matcher and the CPU restatement of the reference GpSM pipeline. Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg import this package;
+the product (gpsm_b200, libgpsm.so) never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+REF_OK, REF_EMPTY_INIT, REF_EMPTY_REFINE, REF_EMPTY_JOIN = 0, 1, 2, 3
+REF_DISCONNECTED, REF_NO_EDGES, REF_EMPTY_CEDGE = 4, 5, 6
+
+vp, u32, u64, i32, i64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
+_SIG = {
+    "oracle_enumerate": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, u64, vp, u64]),
+    "oracle_ref_plan": (vp, [u32, vp, vp, vp, u32, vp, u32, vp, vp]),
+    "oracle_ref_free": (None, [vp]),
+    "oracle_ref_info": (None, [vp, vp, vp, vp, vp]),
+    "oracle_ref_edges": (None, [vp, vp, vp]),
+    "oracle_ref_order": (None, [vp, vp]),
+    "oracle_ref_cand": (C.c_int, [vp, C.c_int, vp]),
+    "oracle_ref_cedge_sizes": (None, [vp, vp, vp, vp, vp]),
+    "oracle_ref_cedge_len": (u64, [vp, u32, C.c_int]),
+    "oracle_ref_cedge_copy": (None, [vp, u32, C.c_int, vp]),
+    "oracle_ref_steps": (None, [vp, vp, vp, vp]),
+    "oracle_ref_mapping": (None, [vp, vp, vp]),
+    "oracle_ref_join": (i64, [vp, C.c_int, u64, vp, vp, u64, vp, u64]),
+    "oracle_ref_verify": (C.c_int, [vp, vp, vp, u64, vp]),
+    "oracle_cpu_pipeline": (C.c_double, [u32, vp, vp, vp, u32, vp, vp, vp, vp, C.c_int, u64, vp, C.c_double]),
+}
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = C.CDLL(LIB_PATH)
+        for k, (r, a) in _SIG.items():
+            f = getattr(lib, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(vp)
+
+
+def _u32(x):
+    return np.ascontiguousarray(x, dtype=np.uint32)
+
+
+def enumerate_embeddings(g, q, cap=1 << 62, rows=True, out_cap=None):
+    """Sorted embeddings (rows indexed by query vertex) and their count."""
+    lib = load()
+    qe = _u32(q.edges).reshape(-1)
+    if rows:
+        if out_cap is None:
+            cnt = lib.oracle_enumerate(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
+                                       q.m, _p(qe), cap, None, 0)
+            out_cap = cnt
+        out = np.zeros((max(out_cap, 1), q.n), dtype=np.uint32)
+        cnt = lib.oracle_enumerate(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
+                                   q.m, _p(qe), cap, _p(out), out_cap)
+        return out[: min(cnt, out_cap)], cnt
+    cnt = lib.oracle_enumerate(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
+                               q.m, _p(qe), cap, None, 0)
+    return None, cnt
+
+
+class RefPlan:
+    """CPU restatement of the reference pipeline for one (graph, query)."""
+
+    def __init__(self, g, q):
+        self.lib = load()
+        self.g, self.q = g, q
+        st = C.c_int32(0)
+        self._ql = _u32(q.labels)
+        self._qe = _u32(q.edges).reshape(-1)
+        self.h = self.lib.oracle_ref_plan(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(self._ql),
+                                          q.m, _p(self._qe), C.byref(st))
+        self.status = st.value
+        m, ns, de, no = u32(0), u32(0), i32(0), u32(0)
+        self.lib.oracle_ref_info(self.h, C.byref(m), C.byref(ns), C.byref(de), C.byref(no))
+        self.m, self.nsteps, self.defect, self.norder = m.value, ns.value, de.value, no.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_ref_free(self.h)
+            self.h = None
+
+    def edges(self):
+        f = np.zeros(self.m, np.uint32)
+        t = np.zeros(self.m, np.uint32)
+        self.lib.oracle_ref_edges(self.h, _p(f), _p(t))
+        return f, t
+
+    def filter_order(self):
+        o = np.zeros(self.norder, np.uint32)
+        self.lib.oracle_ref_order(self.h, _p(o))
+        return o
+
+    def candidates(self, which=1):
+        out = np.zeros((self.q.n, self.g.n), np.uint8)
+        if self.lib.oracle_ref_cand(self.h, which, _p(out)) != 0:
+            return None
+        return out.astype(bool)
+
+    def cedge_sizes(self):
+        sf = np.zeros(self.m, np.uint64)
+        nf = np.zeros(self.m, np.uint32)
+        sr = np.zeros(self.m, np.uint64)
+        nr = np.zeros(self.m, np.uint32)
+        self.lib.oracle_ref_cedge_sizes(self.h, _p(sf), _p(nf), _p(sr), _p(nr))
+        return sf, nf, sr, nr
+
+    def cedge(self, e, rev=False):
+        n = self.lib.oracle_ref_cedge_len(self.h, e, int(rev))
+        out = np.zeros(n, np.uint32)
+        self.lib.oracle_ref_cedge_copy(self.h, e, int(rev), _p(out))
+        return out
+
+    def steps(self):
+        e = np.zeros(self.nsteps, np.uint32)
+        mo = np.zeros(self.nsteps, np.int32)
+        de = np.zeros(self.nsteps, np.int32)
+        self.lib.oracle_ref_steps(self.h, _p(e), _p(mo), _p(de))
+        return e, mo, de
+
+    def mapping(self):
+        a = np.zeros(self.q.n, np.int32)
+        b = np.zeros(self.q.n, np.int32)
+        self.lib.oracle_ref_mapping(self.h, _p(a), _p(b))
+        return a, b  # id2pos, pos2id
+
+    def join(self, injective=True, cap=1 << 62, rows=True, out_cap=None, work_cap=0):
+        """(rows in table-column order or None, count, per-step row counts, capped)."""
+        lv = np.zeros(max(self.nsteps, 1), np.uint64)
+        capped = C.c_int(0)
+        if rows:
+            if out_cap is None:
+                cnt = self.lib.oracle_ref_join(self.h, int(injective), cap, _p(lv), None, 0, C.byref(capped), work_cap)
+                out_cap = cnt
+            out = np.zeros((max(out_cap, 1), self.q.n), np.uint32)
+            cnt = self.lib.oracle_ref_join(self.h, int(injective), cap, _p(lv), _p(out), out_cap,
+                                           C.byref(capped), work_cap)
+            return out[: min(cnt, out_cap)], cnt, lv[: self.nsteps], bool(capped.value)
+        cnt = self.lib.oracle_ref_join(self.h, int(injective), cap, _p(lv), None, 0, C.byref(capped), work_cap)
+        return None, cnt, lv[: self.nsteps], bool(capped.value)
+
+
+DEADLINE_STOPPED = np.iinfo(np.int64).min
+
+
+def cpu_pipeline(g, queries, threads=None, cap=1 << 62, deadline_s=0.0):
+    """CPU port of the whole path over a query list: (counts, seconds).
+    counts[k] == DEADLINE_STOPPED when the deadline stopped query k."""
+    lib = load()
+    threads = threads or os.cpu_count() or 1
+    voff = np.zeros(len(queries) + 1, np.uint32)
+    eoff = np.zeros(len(queries) + 1, np.uint64)
+    for i, q in enumerate(queries):
+        voff[i + 1] = voff[i] + q.n
+        eoff[i + 1] = eoff[i] + q.m
+    ql = np.concatenate([_u32(q.labels) for q in queries]) if queries else np.zeros(1, np.uint32)
+    qe = np.concatenate([_u32(q.edges).reshape(-1) for q in queries]) if queries else np.zeros(2, np.uint32)
+    qe = _u32(qe)
+    counts = np.zeros(len(queries), np.int64)
+    secs = lib.oracle_cpu_pipeline(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), len(queries), _p(voff),
+                                   _p(_u32(ql)), _p(eoff), _p(qe), threads, cap, _p(counts), float(deadline_s))
+    return counts, secs

@@ -1,0 +1,180 @@
+"""GPU parity: every product of the CUDA path against the oracle.
+
+Filter stage (candidate sets, candidate-edge totals, filter order, plain
+join order) is compared bit for bit with the restated reference pipeline;
+embeddings are compared row for row (same table order) with the restated
+joins and as sets with the independent backtracking oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from gpsm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(n, edges, labels):
+    return W.graph_from_edges(n, np.array(edges, np.uint32).reshape(-1, 2), np.array(labels, np.uint32))
+
+
+def _query(labels, edges):
+    return W.Query(np.array(labels, np.uint32), np.array(edges, np.uint32).reshape(-1, 2))
+
+
+def _sorted_rows(a):
+    return sorted(map(tuple, np.asarray(a).tolist()))
+
+
+def check_filter(G, dg, g, q):
+    d = G.debug_filter(dg, q, with_candidates=True)
+    plan = oracle.RefPlan(g, q)
+    assert list(d["filter_order"][: plan.norder]) == list(plan.filter_order())
+    if plan.status != oracle.REF_OK:
+        assert d["empty"]
+        return plan, d
+    assert not d["empty"]
+    assert np.array_equal(d["candidates"], plan.candidates(1))
+    sf, nf, sr, nr = plan.cedge_sizes()
+    assert np.array_equal(d["size_fwd"], sf)
+    assert np.array_equal(d["size_rev"], sr)
+    assert np.array_equal(d["cand_count"], plan.candidates(1).sum(axis=1))
+    _, pos2id = plan.mapping()
+    assert np.array_equal(d["plain_pos2id"], pos2id)
+    return plan, d
+
+
+@pytest.fixture(scope="module")
+def small_dg(gpu, small_er):
+    return gpu.DeviceGraph(small_er.graph)
+
+
+def test_filter_stage_matches_reference_small_er(gpu, small_er, small_dg):
+    for q in small_er.queries:
+        check_filter(gpu, small_dg, small_er.graph, q)
+
+
+def test_embeddings_match_small_er(gpu, small_er, small_dg):
+    g = small_er.graph
+    for q in small_er.queries:
+        out = gpu.match(small_dg, q)
+        plan = oracle.RefPlan(g, q)
+        ref_rows, ref_cnt, _, _ = plan.join(injective=True)
+        id2pos, _ = plan.mapping()
+        assert out.count == ref_cnt and not out.capped
+        assert np.array_equal(out.id_map, id2pos)
+        assert np.array_equal(out.rows, ref_rows)  # same table order as the reference
+        rows, cnt = oracle.enumerate_embeddings(g, q)
+        assert cnt == out.count
+        assert _sorted_rows(out.embeddings()) == [tuple(x) for x in rows.tolist()]
+
+
+def test_level_chunking_and_result_spill_keep_order(gpu, small_er, small_dg):
+    q = small_er.queries[1]
+    full = gpu.match(small_dg, q)
+    tiny = gpu.match(small_dg, q, level_bytes=4096, result_rows=64)
+    assert np.array_equal(full.rows, tiny.rows)
+
+
+def test_cap_gives_first_rows_in_order(gpu, small_er, small_dg):
+    g = small_er.graph
+    for q in small_er.queries[:4]:
+        plan = oracle.RefPlan(g, q)
+        ref_rows, _, _, _ = plan.join(injective=True, cap=333)
+        out = gpu.match(small_dg, q, cap=333)
+        assert out.capped and out.count == 333
+        assert np.array_equal(out.rows, ref_rows)
+
+
+def test_count_only(gpu, small_er, small_dg):
+    q = small_er.queries[2]
+    a = gpu.match(small_dg, q)
+    b = gpu.match(small_dg, q, count_only=True)
+    assert b.rows is None and b.count == a.count
+
+
+def test_given_orders_give_the_same_set(gpu, small_er, small_dg):
+    rng = np.random.default_rng(0)
+    for q in small_er.queries[:5]:
+        base = gpu.match(small_dg, q)
+        adj = {i: set() for i in range(q.n)}
+        for a, b in q.edges:
+            adj[int(a)].add(int(b))
+            adj[int(b)].add(int(a))
+        for _ in range(3):
+            order = [int(rng.integers(q.n))]
+            while len(order) < q.n:
+                cand = sorted({w for u in order for w in adj[u]} - set(order))
+                order.append(cand[int(rng.integers(len(cand)))])
+            out = gpu.match(small_dg, q, order=order)
+            assert np.array_equal(out.pos2id, order)
+            assert _sorted_rows(out.embeddings()) == _sorted_rows(base.embeddings())
+
+
+def test_invalid_order_is_rejected(gpu, small_er, small_dg):
+    q = small_er.queries[0]
+    with pytest.raises(gpu.GpsmError):
+        gpu.match(small_dg, q, order=[0] * q.n)
+
+
+def test_edge_cases(gpu):
+    # triangle in K4
+    g = _graph(4, [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)], [1, 1, 1, 1])
+    dg = gpu.DeviceGraph(g)
+    out = gpu.match(dg, _query([1, 1, 1], [(0, 1), (1, 2), (0, 2)]))
+    assert out.count == 24
+    # single-vertex query: every vertex with the label
+    g2 = _graph(5, [(0, 1), (1, 2)], [1, 2, 1, 1, 2])
+    dg2 = gpu.DeviceGraph(g2)
+    out = gpu.match(dg2, _query([1], []))
+    assert _sorted_rows(out.embeddings()) == [(0,), (2,), (3,)]
+    # absent label
+    out = gpu.match(dg2, _query([1, 7], [(0, 1)]))
+    assert out.count == 0 and out.empty_filter
+    # one edge
+    out = gpu.match(dg2, _query([1, 2], [(0, 1)]))
+    assert _sorted_rows(out.embeddings()) == [(0, 1), (2, 1)]
+    # disconnected query is rejected
+    with pytest.raises(gpu.GpsmError):
+        gpu.match(dg2, _query([1, 2, 1], [(0, 1)]))
+    # parallel data edges: each embedding once
+    g3 = _graph(3, [(0, 1), (0, 1), (1, 2)], [1, 1, 1])
+    dg3 = gpu.DeviceGraph(g3)
+    out = gpu.match(dg3, _query([1, 1], [(0, 1)]))
+    assert _sorted_rows(out.embeddings()) == [(0, 1), (1, 0), (1, 2), (2, 1)]
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_graphs_against_backtracking(gpu, seed):
+    g = W.rmat_graph(12, 24000, 12, 1.0, seed=seed)
+    dg = gpu.DeviceGraph(g)
+    for k in range(4):
+        q = W.random_walk_query(g, 5 + k, 1000 * seed + k, W.MODE_DENSE if k % 2 else W.MODE_TREE, 0.5)
+        check_filter(gpu, dg, g, q)
+        rows, cnt = oracle.enumerate_embeddings(g, q, cap=200000)
+        out = gpu.match(dg, q, cap=200000)
+        plan = oracle.RefPlan(g, q)
+        ref_rows, ref_cnt, _, _ = plan.join(injective=True, cap=200000)
+        assert out.count == ref_cnt
+        assert np.array_equal(out.rows, ref_rows)
+        if cnt < 200000:
+            assert _sorted_rows(out.embeddings()) == [tuple(x) for x in rows.tolist()]
+
+
+@pytest.fixture(scope="module")
+def rmat20(gpu):
+    wl = W.workload("rmat20", count=6)
+    return wl, gpu.DeviceGraph(wl.graph)
+
+
+def test_rmat20_filter_and_capped_rows(gpu, rmat20):
+    wl, dg = rmat20
+    g = wl.graph
+    for q in wl.queries[:4]:
+        plan, _ = check_filter(gpu, dg, g, q)
+        ref_rows, ref_cnt, _, capped = plan.join(injective=True, cap=50000, work_cap=int(5e7))
+        out = gpu.match(dg, q, cap=50000)
+        if capped and ref_cnt < 50000:
+            continue  # oracle stopped on its work bound, not on the cap
+        assert out.count == ref_cnt
+        assert np.array_equal(out.rows, ref_rows)

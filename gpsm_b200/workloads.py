@@ -190,3 +190,50 @@ def workload(name, seed=0, count=None):
     else:
         raise ValueError(name)
     return Workload(name, g, qs)
+
+
+def write_text(path, graphs, append=False, terminate=True, first_id=0):
+    """Write graphs in the reference's text format (io/IO.cpp:87-142):
+    't # id', a count line 'n m vertex_labels edge_labels', 'v i label' per
+    vertex, 'e from to 1' per edge; the file ends with 't # -1' (without it
+    the reference's reader loops at end of file). Each undirected edge is
+    written once. graphs: iterable of (labels, edges)."""
+    mode = "a" if append else "w"
+    with open(path, mode) as f:
+        for k, (labels, edges) in enumerate(graphs):
+            labels = np.asarray(labels, np.uint32)
+            edges = np.asarray(edges, np.uint32).reshape(-1, 2)
+            n, m = len(labels), len(edges)
+            f.write(f"t # {first_id + k}\n{n} {m} {len(np.unique(labels))} 1\n")
+            if n:
+                f.write("\n".join(f"v {i} {int(x)}" for i, x in enumerate(labels)) + "\n")
+            if m:
+                f.write("\n".join(f"e {int(a)} {int(b)} 1" for a, b in edges) + "\n")
+        if terminate:
+            f.write("t # -1\n")
+
+
+def read_text(path):
+    """Read every graph of a reference-format text file: [(labels, edges)]."""
+    out = []
+    labels, edges = None, None
+    with open(path) as f:
+        for line in f:
+            p = line.split()
+            if not p:
+                continue
+            if p[0] == "t":
+                if labels is not None:
+                    out.append((np.array(labels, np.uint32), np.array(edges, np.uint32).reshape(-1, 2)))
+                if int(p[2]) == -1:
+                    labels = None
+                    break
+                labels, edges = [], []
+                next(f)  # count line
+            elif p[0] == "v":
+                labels.append(int(p[2]))
+            elif p[0] == "e":
+                edges.append((int(p[1]), int(p[2])))
+    if labels is not None:
+        out.append((np.array(labels, np.uint32), np.array(edges, np.uint32).reshape(-1, 2)))
+    return out

@@ -26,6 +26,9 @@ CUFLAGS = ARCH + ["-lineinfo", "--expt-relaxed-constexpr"]
 def _sources():
     cu = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
     cpp = sorted(f for f in os.listdir(CSRC) if f.endswith(".cpp") and f != "gpsm_run.cpp")
+    host = os.path.join(CSRC, "host")
+    if os.path.isdir(host):
+        cpp += sorted(os.path.join("host", f) for f in os.listdir(host) if f.endswith(".cpp"))
     return cu, cpp
 
 
@@ -47,11 +50,12 @@ def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     cu, cpp = _sources()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    headers += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    for d, _, fs in os.walk(INCLUDE):
+        headers += [os.path.join(d, f) for f in fs]
     objs = []
     for f in cu + cpp:
         src = os.path.join(CSRC, f)
-        obj = os.path.join(BUILD, f + ".o")
+        obj = os.path.join(BUILD, f.replace(os.sep, "_") + ".o")
         objs.append(obj)
         if force or _newer(obj, [src] + headers):
             flags = COMMON + (CUFLAGS if f.endswith(".cu") else ["-x", "c++"])

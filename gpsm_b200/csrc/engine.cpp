@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <queue>
 
@@ -209,6 +211,15 @@ bool valid_order(const QueryPlan& Q, const std::vector<int32_t>& pos2id) {
 }
 
 namespace {
+
+bool trace_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("GPSM_TRACE");
+    on = (e && *e && *e != '0') ? 1 : 0;
+  }
+  return on == 1;
+}
 
 template <class T>
 T* arena_alloc(Workspace& ws, uint64_t count) {
@@ -466,9 +477,17 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
   if (!hb.empty())
     GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
-  ExpandResult* d_res = arena_alloc<ExpandResult>(ws, 1);
-  ExpandResult* h_res = reinterpret_cast<ExpandResult*>(ws.h_small + 1024);
-  ExpandResult* h_init = reinterpret_cast<ExpandResult*>(ws.h_small + 1032);
+  StepState* d_st = arena_alloc<StepState>(ws, 1);
+  StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
+  JoinScratch js;
+  uint32_t max_nb = 1;
+  for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
+  // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
+  js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
+  js.rng_entries = js.rows * max_nb;
+  js.drv = arena_alloc<uint4>(ws, js.rows);
+  js.rng = arena_alloc<uint4>(ws, js.rng_entries);
+  js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
   GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
   R.stats.level_rows.assign(qn + 1, 0);
@@ -525,7 +544,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     emitted = n1;
     R.stats.level_rows[1] = n1;
   }
-  uint64_t exp_launches = 0, driver_elems = 0;
+  uint64_t exp_launches = 0;
   uint64_t alg_bytes = 0;
   while (qn > 1 && !capped) {
     // deepest level with rows left
@@ -539,24 +558,19 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     Level& A = L[lv];
     const bool final_level = (uint32_t)lv + 1 == qn;
     uint32_t* out;
-    uint64_t out_cap;
+    uint64_t out_cap, budget;
     bool partial = false;
     if (final_level) {
       uint64_t space = res_cap - res_used;
-      if (space == 0) {
-        if (opt.keep_on_device) {
-          set_last_error("device result buffer full");
-          return GPSM_ERR_BUDGET;
-        }
-        flush();
-        space = res_cap;
-      }
       out = res_buf + res_used * qn;
       if (cap - emitted <= space) {
+        // the cap ends the query inside this buffer: rows past it are cut
         out_cap = cap - emitted;
         partial = true;
+        budget = std::min<uint64_t>(std::max<uint64_t>(out_cap, min_rows), opt.step_cands);
       } else {
         out_cap = space;
+        budget = std::min<uint64_t>(space, opt.step_cands);
       }
     } else {
       Level& B = L[lv + 1];
@@ -564,65 +578,61 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       B.next = 0;
       out = B.buf;
       out_cap = B.cap_rows;
+      budget = std::min<uint64_t>(out_cap, opt.step_cands);
     }
-    uint64_t want = (uint64_t)((double)out_cap / std::max(A.ratio, 1.0 / 64.0));
-    want = std::max<uint64_t>(want, 64);
-    want = std::min<uint64_t>(want, (uint64_t)ws.scan.max_tiles * 64);
+    // rows offered to this step: enough to fill the budget at the observed
+    // candidates per row, within the per-row scratch
+    uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
+    want = std::min<uint64_t>(want, js.rows);
     const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
-    h_init->total = 0;
-    h_init->cut_pos = ~0ULL;
-    h_init->cut_row = ~0ULL;
-    h_init->driver = 0;
-    GPSM_CUDA(cudaMemcpyAsync(d_res, h_init, sizeof(ExpandResult), cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
     GPSM_CUDA(cudaEventRecord(ws.eve0, s));
-    launch_expand(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], out, out_cap, partial, d_res,
-                  nbrs_total);
+    launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
+                     out_cap, js, d_st);
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
-    ++exp_launches;
-    GPSM_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(ExpandResult), cudaMemcpyDeviceToHost, s));
+    exp_launches += 2;
+    GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
     GPSM_CUDA(cudaStreamSynchronize(s));
     {
       float ems = 0;
       GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
       R.stats.expand_ms += ems;
     }
-    uint64_t written, consumed_end;
-    if (h_res->cut_row != ~0ULL) {
-      written = h_res->cut_pos;
-      consumed_end = h_res->cut_row;
-    } else {
-      written = std::min<uint64_t>(h_res->total, out_cap);
-      consumed_end = re;
+    const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
+    if (trace_enabled()) {
+      float ems = 0;
+      cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
+      fprintf(stderr, "[gpsm] step level=%d rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu ms=%.3f\n",
+              lv, (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
+              (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ems);
     }
-    driver_elems += h_res->driver;
-    const uint64_t consumed = consumed_end - rb;
-    alg_bytes += consumed * 4ull * lv + written * 4ull * (lv + 1);
-    if (consumed > 0) A.ratio = std::max(1.0 / 64.0, (double)h_res->total / (double)(re - rb));
-    if (consumed == 0 && written == 0 && !final_level) {
-      set_last_error("a single row produced more rows than a level buffer holds");
-      return GPSM_ERR_BUDGET;
-    }
-    A.next = consumed_end;
-    R.stats.level_rows[lv + 1] += written;
-    if (final_level) {
-      res_used += written;
-      emitted += written;
-      if (emitted >= cap) capped = true;
-      if (!capped && h_res->cut_row != ~0ULL) {
-        // buffer full: drain it and resume from the cut row
+    if (admitted == 0) {
+      if (final_level && !partial && res_used > 0) {  // make room and retry
         if (opt.keep_on_device) {
           set_last_error("device result buffer full");
           return GPSM_ERR_BUDGET;
         }
         flush();
+        continue;
       }
+      set_last_error("a single row has more candidates than a join step admits");
+      return GPSM_ERR_BUDGET;
+    }
+    A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
+    A.next = rb + admitted;
+    alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
+    R.stats.level_rows[lv + 1] += written;
+    if (final_level) {
+      res_used += written;
+      emitted += written;
+      if (emitted >= cap) capped = true;
     } else {
       L[lv + 1].nrows = written;
     }
   }
   if (emitted >= cap) capped = true;
   R.stats.expand_launches = exp_launches;
-  R.stats.alg_bytes_join = alg_bytes + driver_elems * 4;
+  R.stats.alg_bytes_join = alg_bytes;
   R.rows = emitted;
   R.capped = capped;
   GPSM_CUDA(cudaEventRecord(ws.ev1, s));

@@ -46,6 +46,8 @@ struct MatchOptions {
   std::vector<int32_t> given_order;  // pos2id when ORDER_GIVEN
   uint64_t level_bytes = 256ull << 20;  // per intermediate level buffer
   uint64_t result_rows = 1ull << 22;    // device result buffer rows before flushing to host
+  uint64_t step_rows = 1ull << 22;      // input rows one join step may look at
+  uint64_t step_cands = 1ull << 25;     // candidates one join step may admit
   bool keep_on_device = false;          // never flush: fail with GPSM_ERR_BUDGET instead
   bool collect_rows = true;             // false: count only (result rows are discarded)
   bool filter_only = false;             // stop after the join order (debug entry points)

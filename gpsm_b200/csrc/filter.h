@@ -52,20 +52,34 @@ struct BackNbr {
 
 constexpr uint32_t kMaxBack = 128;  // query vertices are < 128 here; checked on the host
 
-struct ExpandResult {  // device-side result words of one expand launch
-  unsigned long long total;     // sum of row output counts over all input rows processed
-  unsigned long long cut_pos;   // output position of the first row not written (~0 = none)
-  unsigned long long cut_row;   // first input row not written (~0 = none)
-  unsigned long long driver;    // sum over rows of the driving list length (pass 1)
+// Device-side bookkeeping of one join step (initialised by the host).
+struct StepState {
+  unsigned long long rows;         // input rows admitted (a prefix of the step's rows)
+  unsigned long long written;      // output rows written (<= out_cap)
+  unsigned long long done;         // set once the output reached out_cap
+  unsigned long long blocks_done;  // persistent blocks finished
+  unsigned long long cands;        // candidates of the admitted rows
+  unsigned long long pad;
 };
 
-// Expands input rows [row_begin, row_end) (in_cols columns, row-major) by one
-// query vertex whose placed neighbours are `back[0..nb)`. Outputs go to
-// `out` (in_cols+1 columns) up to out_cap rows; when `partial` is set the
-// last row may be cut inside (embedding cap). res must be initialised.
-// nbrs_total bounds every candidate-edge range (a failed check raises DF_BOUNDS).
-void launch_expand(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
-                   const BackNbr* d_back, uint32_t nb, uint32_t* out, uint64_t out_cap, bool partial,
-                   ExpandResult* d_res, uint64_t nbrs_total);
+// Per-row scratch of a join step: driver list (lo, hi32 of lo, length, j)
+// and candidate offsets (rows + 1 entries).
+struct JoinScratch {
+  uint4* drv = nullptr;
+  uint4* rng = nullptr;               // rows x nb list ranges (lo, lo>>32, length, 0)
+  unsigned long long* coff = nullptr;
+  uint64_t rows = 0;
+  uint64_t rng_entries = 0;
+};
+
+// One join step over input rows [row_begin, row_end) (in_cols columns,
+// row-major): rows are admitted in order while their candidates fit
+// `budget`; admitted rows are extended by the query vertex whose placed
+// neighbours are back[0..nb) into `out` (in_cols+1 columns), at most out_cap
+// rows (the first out_cap in order). nbrs_total bounds every list range.
+void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
+                      const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st);
+uint64_t join_rows_per_locate_tile();
 
 }  // namespace gpsm

@@ -1,30 +1,35 @@
-// Join kernels: one launch extends a range of partial embeddings (rows of a
-// row-major table) by one query vertex.
+// Join kernels: one step extends a range of partial embeddings (rows of a
+// row-major table) by one query vertex v and checks all of v's edges to
+// already-placed vertices at once.
 //
 // The reference joins one query edge at a time (match/Match.cu:1141-1569):
 // table_kernel seeds pairs, expand_kernel + link_kernel add a column for a
 // tree edge, join_kernel + filter_kernel drop rows failing a non-tree edge.
-// Every one of those kernels finds mu in the candidate list by a warp-wide
-// LINEAR scan of C(u) per row, and no kernel checks injectivity (the host
-// filters afterwards, io/IO.cpp:187-222).
+// Each of those kernels finds mu in the candidate list by a warp-wide
+// LINEAR scan of C(u) per row, runs one warp per row whatever the row's
+// list length, and none checks injectivity (io/IO.cpp:187-222 filters on the
+// host afterwards).
 //
-// Here a vertex v and all of its edges to already-placed vertices are joined
-// in one pass:
-//   - the candidate-edge list of every placed neighbour w is located in O(1)
-//     with a rank lookup in C(w)'s bitmap (no scan of C(w));
-//   - the shortest of those lists drives the row; every other list is probed
-//     by binary search (sorted-adjacency intersection);
-//   - a candidate equal to a data vertex already in the row is dropped
-//     (injectivity), so no homomorphism rows are ever materialised.
-// The rows a vertex order produces are the reference's rows after its
-// non-tree checks for that vertex, minus the non-injective ones, in the same
-// order: input rows in order, each row's candidates ascending.
-//
-// Output positions come from a single-pass decoupled look-back over 64-row
-// tiles, so the table stays in order without a separate scan launch. When
-// the output buffer would overflow, the first row that does not fit and
-// every later row are left for a later launch (cut_row); with `partial` set
-// (the embedding cap) the crossing row is cut inside instead.
+// Here a step is two kernels:
+//   k_locate  (one thread per input row) finds, for every placed neighbour
+//             w of v, the candidate-edge list N(row[w]) ∩ C(v) with an O(1)
+//             rank lookup in C(w)'s bitmap, keeps the shortest one as the
+//             row's driver, and turns the driver lengths into candidate
+//             offsets with a single-pass decoupled look-back scan. Rows are
+//             admitted in order while their candidates fit the step budget.
+//   k_extend  (one thread per candidate, persistent blocks) takes candidate
+//             t of row r from the driver list and keeps it if it differs
+//             from every value in the row (injectivity) and lies in every
+//             other placed neighbour's list (binary search: sorted-list
+//             intersection). Kept candidates are compacted in order with a
+//             warp ballot and a decoupled look-back over 1024-candidate
+//             tiles; each warp writes its output rows as one contiguous,
+//             coalesced span.
+// Work is spread by candidate, not by row, so a hub row with 60k candidates
+// and a row with one candidate cost the same per candidate. The output keeps
+// the reference's row order (input rows in order, each row's candidates
+// ascending), and the output never overflows: a step admits rows only while
+// their candidate count (an upper bound on outputs) fits the buffer.
 #include <cuda_runtime.h>
 
 #include "filter.h"
@@ -32,16 +37,17 @@
 
 namespace gpsm {
 
-constexpr int kExpBlock = 256;
-constexpr int kExpWarps = kExpBlock / 32;
-constexpr int kExpRowsPerWarp = 8;
-constexpr int kExpTile = kExpWarps * kExpRowsPerWarp;  // 64 rows per tile
+constexpr int kLocBlock = 256;  // rows per locate tile
+constexpr int kExtBlock = 256;
+constexpr int kExtItems = 4;
+constexpr int kExtTile = kExtBlock * kExtItems;  // candidates per extend tile
+constexpr uint32_t kExtGrid = 148 * 8;           // persistent extend blocks
 
 __device__ __forceinline__ bool sorted_contains(const uint32_t* __restrict__ a, unsigned long long lo,
                                                 unsigned long long hi, uint32_t key) {
   while (lo < hi) {
-    unsigned long long mid = (lo + hi) >> 1;
-    uint32_t x = a[mid];
+    const unsigned long long mid = (lo + hi) >> 1;
+    const uint32_t x = __ldg(a + mid);
     if (x == key) return true;
     if (x < key) lo = mid + 1;
     else hi = mid;
@@ -49,186 +55,244 @@ __device__ __forceinline__ bool sorted_contains(const uint32_t* __restrict__ a, 
   return false;
 }
 
-struct ExpandShared {
-  BackNbr back[kMaxBack];
-  uint32_t row[kExpWarps][kMaxBack];
-  unsigned long long lo[kExpWarps][kMaxBack];
-  unsigned long long hi[kExpWarps][kMaxBack];
-  uint32_t cnt[kExpTile];
-  unsigned long long off[kExpTile];
-  uint32_t tile;
-  uint32_t cut;
-  unsigned long long prefix;
-  unsigned long long driver;
-  unsigned long long nbrs_total;
-  uint32_t* flags;
-};
-
-// Processes one row with the calling warp. write=false: returns the number
-// of accepted candidates. write=true: writes them starting at output
-// position pos (rows at positions >= out_cap are skipped).
-__device__ __forceinline__ uint32_t expand_row(ExpandShared& S, uint32_t w, const uint32_t* __restrict__ in,
-                                               uint32_t cols, unsigned long long r, uint32_t nb, bool write,
-                                               uint32_t* __restrict__ out, unsigned long long pos,
-                                               unsigned long long out_cap, unsigned long long* driver_len) {
-  const uint32_t lane = threadIdx.x & 31;
-  uint32_t* row = S.row[w];
-  const uint32_t* src = in + r * cols;
-  for (uint32_t k = lane; k < cols; k += 32) row[k] = src[k];
-  __syncwarp();
-  // locate every placed neighbour's candidate list for its data vertex
-  unsigned long long best_len = ~0ULL;
-  uint32_t best_j = 0;
-  for (uint32_t j = lane; j < nb; j += 32) {
-    const BackNbr& b = S.back[j];
-    const uint32_t mu = row[b.col];
-    const uint32_t word = mu >> 5, bit = mu & 31;
-    const uint32_t bw = b.bm[word];
-    const uint32_t idx = b.rank[word] + __popc(bw & ((1u << bit) - 1u));
-    unsigned long long lo = 0, hi = 0;
-    if ((bw >> bit) & 1u) {  // every table value is a candidate of its column's vertex
-      lo = b.off[idx];
-      hi = b.off[idx + 1];
-    }
-    if (hi < lo || hi > S.nbrs_total || !((bw >> bit) & 1u)) {
-      atomicOr(S.flags, (uint32_t)DF_BOUNDS);
-      lo = hi = 0;
-    }
-    S.lo[w][j] = lo;
-    S.hi[w][j] = hi;
-    if (hi - lo < best_len) {
-      best_len = hi - lo;
-      best_j = j;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long ol = __shfl_xor_sync(0xffffffffu, best_len, o);
-    uint32_t oj = __shfl_xor_sync(0xffffffffu, best_j, o);
-    if (ol < best_len || (ol == best_len && oj < best_j)) {
-      best_len = ol;
-      best_j = oj;
-    }
-  }
-  __syncwarp();
-  const uint32_t d = best_j;
-  const unsigned long long lo = S.lo[w][d], hi = S.hi[w][d];
-  *driver_len = hi - lo;
-  const uint32_t* __restrict__ nd = S.back[d].nbrs;
-  uint32_t count = 0;
-  uint32_t prev_last = 0xffffffffu;
-  const uint32_t out_cols = cols + 1;
-  for (unsigned long long base = lo; base < hi; base += 32) {
-    const unsigned long long k = base + lane;
-    const bool valid = k < hi;
-    uint32_t y = valid ? nd[k] : 0xffffffffu;
-    uint32_t p = __shfl_up_sync(0xffffffffu, y, 1);
-    if (lane == 0) p = prev_last;
-    bool ok = valid && !(k > lo && y == p);  // parallel data edges: one candidate
-    const unsigned long long last = (hi - base < 32) ? (hi - base - 1) : 31;
-    prev_last = __shfl_sync(0xffffffffu, y, (int)last);
-    if (ok) {
-      for (uint32_t c = 0; c < cols; ++c)
-        if (row[c] == y) {
-          ok = false;
-          break;
-        }
-    }
-    if (ok) {
-      for (uint32_t j = 0; j < nb; ++j) {
-        if (j == d) continue;
-        if (!sorted_contains(S.back[j].nbrs, S.lo[w][j], S.hi[w][j], y)) {
-          ok = false;
-          break;
-        }
-      }
-    }
-    const uint32_t bal = __ballot_sync(0xffffffffu, ok);
-    if (write && ok) {
-      const unsigned long long q = pos + count + __popc(bal & ((1u << lane) - 1u));
-      if (q < out_cap) {
-        uint32_t* dst = out + q * out_cols;
-        for (uint32_t c = 0; c < cols; ++c) dst[c] = row[c];
-        dst[cols] = y;
-      }
-    }
-    count += __popc(bal);
-  }
-  __syncwarp();
-  return count;
+// Candidate-edge list of data vertex mu (a candidate of w) towards v.
+__device__ __forceinline__ bool locate_list(const BackNbr& b, uint32_t mu, unsigned long long nbrs_total,
+                                            unsigned long long* lo, unsigned long long* hi) {
+  const uint32_t word = mu >> 5, bit = mu & 31;
+  const uint32_t bw = __ldg(b.bm + word);
+  if (!((bw >> bit) & 1u)) return false;  // every table value is a candidate of its column's vertex
+  const uint32_t idx = __ldg(b.rank + word) + __popc(bw & ((1u << bit) - 1u));
+  *lo = __ldg(b.off + idx);
+  *hi = __ldg(b.off + idx + 1);
+  return *lo <= *hi && *hi <= nbrs_total;
 }
 
-__global__ void __launch_bounds__(kExpBlock) k_expand(const uint32_t* __restrict__ in, uint32_t cols,
-                                                     unsigned long long row_begin, unsigned long long row_end,
+__device__ __forceinline__ void stage_back(BackNbr* dst_back, const BackNbr* __restrict__ back, uint32_t nb) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(back);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(dst_back);
+  const uint32_t words = nb * (uint32_t)(sizeof(BackNbr) / 4);
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+
+struct LocateShared {
+  BackNbr back[kMaxBack];
+  uint32_t tile;
+  unsigned long long prefix;
+};
+
+__global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict__ in, uint32_t cols,
+                                                     unsigned long long row_begin, unsigned long long nrows,
                                                      const BackNbr* __restrict__ back, uint32_t nb,
-                                                     uint32_t* __restrict__ out, unsigned long long out_cap,
-                                                     uint32_t partial, ExpandResult* __restrict__ res,
-                                                     Lookback lb, unsigned long long nbrs_total) {
-  __shared__ ExpandShared S;
-  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    S.tile = lb_take_ticket(lb);
-    S.cut = kExpTile;
-    S.driver = 0;
-    S.nbrs_total = nbrs_total;
-    S.flags = lb.flags;
-  }
-  {
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(back);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(S.back);
-    const uint32_t words = nb * (sizeof(BackNbr) / 4);
-    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
-  }
+                                                     unsigned long long nbrs_total, unsigned long long budget,
+                                                     uint4* __restrict__ drv, uint4* __restrict__ rng,
+                                                     unsigned long long* __restrict__ coff,
+                                                     StepState* __restrict__ st, Lookback lb) {
+  __shared__ LocateShared S;
+  if (threadIdx.x == 0) S.tile = lb_take_ticket(lb);
+  stage_back(S.back, back, nb);
   __syncthreads();
   const uint32_t tile = S.tile;
-  const unsigned long long ntiles = (row_end - row_begin + kExpTile - 1) / kExpTile;
+  const unsigned long long ntiles = (nrows + kLocBlock - 1) / kLocBlock;
   if ((unsigned long long)tile >= ntiles) {  // ticket base out of step with the device counter
     if (threadIdx.x == 0) atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
     return;
   }
-  const unsigned long long first = row_begin + (unsigned long long)tile * kExpTile;
-  const uint32_t nrows = (uint32_t)min((unsigned long long)kExpTile, row_end - first);
-  // pass 1: count accepted candidates per row
-  unsigned long long drv = 0;
-  for (uint32_t i = 0; i < kExpRowsPerWarp; ++i) {
-    const uint32_t rl = wid * kExpRowsPerWarp + i;
-    uint32_t c = 0;
-    unsigned long long dl = 0;
-    if (rl < nrows) c = expand_row(S, wid, in, cols, first + rl, nb, false, out, 0, 0, &dl);
-    drv += dl;
-    if (lane == 0) S.cnt[rl] = c;
+  const unsigned long long i = (unsigned long long)tile * kLocBlock + threadIdx.x;
+  unsigned long long best_lo = 0, best_len = 0;
+  uint32_t best_j = 0;
+  if (i < nrows && nb > 0) {
+    const uint32_t* row = in + (row_begin + i) * cols;
+    best_len = ~0ULL;
+    for (uint32_t j = 0; j < nb; ++j) {
+      unsigned long long lo, hi;
+      if (!locate_list(S.back[j], __ldg(row + S.back[j].col), nbrs_total, &lo, &hi)) {
+        atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
+        lo = hi = 0;
+      }
+      rng[i * nb + j] = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)(hi - lo), 0u);
+      if (hi - lo < best_len) {
+        best_len = hi - lo;
+        best_lo = lo;
+        best_j = j;
+      }
+    }
   }
-  if (lane == 0 && drv) atomicAdd(&S.driver, drv);
-  __syncthreads();
-  if (threadIdx.x == 0 && S.driver) atomicAdd(&res->driver, S.driver);
+  if (i < nrows) drv[i] = make_uint4((uint32_t)best_lo, (uint32_t)(best_lo >> 32), (uint32_t)best_len, best_j);
   unsigned long long total;
-  const unsigned long long mine =
-      block_exclusive_scan<kExpBlock>(threadIdx.x < kExpTile ? S.cnt[threadIdx.x] : 0, &total);
-  if (threadIdx.x < kExpTile) S.off[threadIdx.x] = mine;
-  if (wid == 0) {
-    unsigned long long ex = lb_exclusive(lb, tile, total);
-    if (lane == 0) S.prefix = ex;
+  const unsigned long long mine = block_exclusive_scan<kLocBlock>(best_len, &total);
+  if (threadIdx.x < 32) {
+    const unsigned long long ex = lb_exclusive(lb, tile, total);
+    if (threadIdx.x == 0) S.prefix = ex;
   }
   __syncthreads();
-  const unsigned long long prefix = S.prefix;
-  if (!partial && threadIdx.x < nrows) {
-    if (prefix + S.off[threadIdx.x] + S.cnt[threadIdx.x] > out_cap) atomicMin(&S.cut, threadIdx.x);
+  const unsigned long long off = S.prefix + mine;
+  if (i < nrows) {
+    coff[i] = off;
+    // rows are admitted in order while all their candidates fit the budget
+    if (off + best_len <= budget) atomicMax(&st->rows, i + 1);
+    if (i + 1 == nrows) coff[nrows] = off + best_len;
   }
+}
+
+constexpr uint32_t kSpan = 1024;  // rows of one tile whose offsets are staged in shared memory
+
+struct ExtendShared {
+  BackNbr back[kMaxBack];
+  uint32_t tile;
+  unsigned long long prefix;
+  unsigned long long r0, r1;  // rows holding the tile's first and last candidate
+  uint32_t warp_cnt[kExtItems][kExtBlock / 32];
+  unsigned long long coff[kSpan + 1];
+};
+
+// Row of candidate t: the last row r < nr with coff[r] <= t.
+__device__ __forceinline__ unsigned long long row_of(const unsigned long long* __restrict__ coff,
+                                                     unsigned long long nr, unsigned long long t) {
+  unsigned long long lo = 0, hi = nr;  // coff[lo] <= t < coff[hi]
+  while (hi - lo > 1) {
+    const unsigned long long mid = (lo + hi) >> 1;
+    if (__ldg(coff + mid) <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict__ in, uint32_t cols,
+                                                     unsigned long long row_begin, const BackNbr* __restrict__ back,
+                                                     uint32_t nb, unsigned long long nbrs_total,
+                                                     const uint4* __restrict__ drv, const uint4* __restrict__ rng,
+                                                     const unsigned long long* __restrict__ coff,
+                                                     uint32_t* __restrict__ out, unsigned long long out_cap,
+                                                     StepState* __restrict__ st, Lookback lb,
+                                                     unsigned long long reserved) {
+  __shared__ ExtendShared S;
+  stage_back(S.back, back, nb);
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned long long nr = st->rows;     // rows admitted by k_locate
+  const unsigned long long ncand = nr ? coff[nr] : 0;
+  const unsigned long long ntiles = (ncand + kExtTile - 1) / kExtTile;
+  const uint32_t out_cols = cols + 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) S.tile = lb_take_ticket(lb);
+    __syncthreads();
+    const uint32_t tile = S.tile;
+    if ((unsigned long long)tile >= ntiles) break;
+    const bool skip = *(volatile unsigned long long*)&st->done != 0;  // output cap reached
+    // rows spanned by this tile; their offsets go to shared memory when few
+    const unsigned long long t_first = (unsigned long long)tile * kExtTile;
+    const unsigned long long t_last = min(t_first + kExtTile, ncand) - 1;
+    if (threadIdx.x == 0) {
+      S.r0 = row_of(coff, nr, t_first);
+      S.r1 = row_of(coff, nr, t_last);
+    }
+    __syncthreads();
+    const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
+    const bool staged = span <= kSpan;
+    if (staged)
+      for (uint32_t x = threadIdx.x; x <= span; x += blockDim.x) S.coff[x] = __ldg(coff + r0 + x);
+    __syncthreads();
+    uint32_t keep[kExtItems], yv[kExtItems];
+    unsigned long long rv[kExtItems];
+#pragma unroll
+    for (int k = 0; k < kExtItems; ++k) {
+      const unsigned long long t =
+          (unsigned long long)tile * kExtTile + (unsigned long long)k * kExtBlock + threadIdx.x;
+      keep[k] = 0;
+      yv[k] = 0;
+      rv[k] = 0;
+      if (skip || t >= ncand) continue;
+      unsigned long long r, kk;
+      if (staged) {
+        uint32_t lo_ = 0, hi_ = (uint32_t)span;  // S.coff[lo_] <= t < S.coff[hi_]
+        while (hi_ - lo_ > 1) {
+          const uint32_t mid = (lo_ + hi_) >> 1;
+          if (S.coff[mid] <= t) lo_ = mid;
+          else hi_ = mid;
+        }
+        r = r0 + lo_;
+        kk = t - S.coff[lo_];
+      } else {
+        r = row_of(coff, nr, t);
+        kk = t - __ldg(coff + r);
+      }
+      const uint4 d = __ldg(drv + r);
+      const unsigned long long lo = ((unsigned long long)d.y << 32) | d.x;
+      const uint32_t* __restrict__ nbrs = S.back[d.w].nbrs;
+      const uint32_t y = __ldg(nbrs + lo + kk);
+      rv[k] = r;
+      yv[k] = y;
+      bool ok = !(kk > 0 && __ldg(nbrs + lo + kk - 1) == y);  // parallel data edges: once
+      const uint32_t* row = in + (row_begin + r) * cols;
+      for (uint32_t c = 0; ok && c < cols; ++c) ok = __ldg(row + c) != y;
+      for (uint32_t j = 0; ok && j < nb; ++j) {
+        if (j == d.w) continue;
+        const uint4 g2 = __ldg(rng + r * nb + j);  // list of the row's j-th placed neighbour
+        const unsigned long long l2 = ((unsigned long long)g2.y << 32) | g2.x;
+        ok = sorted_contains(S.back[j].nbrs, l2, l2 + g2.z, y);
+      }
+      keep[k] = ok;
+    }
+    // in-order positions: slice k of the tile precedes slice k+1
+    uint32_t bal[kExtItems];
+#pragma unroll
+    for (int k = 0; k < kExtItems; ++k) {
+      bal[k] = __ballot_sync(0xffffffffu, keep[k]);
+      if (lane == 0) S.warp_cnt[k][wid] = __popc(bal[k]);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      unsigned long long run = 0;
+#pragma unroll
+      for (int k = 0; k < kExtItems; ++k) {
+        const uint32_t v = lane < kExtBlock / 32 ? S.warp_cnt[k][lane] : 0;
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= (uint32_t)o) x += y;
+        }
+        const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+        if (lane < kExtBlock / 32) S.warp_cnt[k][lane] = (uint32_t)run + x - v;
+        run += tot;
+      }
+      const unsigned long long ex = lb_exclusive(lb, tile, run);
+      if (lane == 0) {
+        S.prefix = ex;
+        if (ex + run >= out_cap) atomicExch(&st->done, 1ULL);
+        if ((unsigned long long)tile == ntiles - 1) st->written = min(ex + run, out_cap);
+      }
+    }
+    __syncthreads();
+    const unsigned long long prefix = S.prefix;
+    if (prefix >= out_cap) continue;
+    // each warp's kept rows of slice k are one contiguous span of the output
+#pragma unroll
+    for (int k = 0; k < kExtItems; ++k) {
+      const uint32_t n = __popc(bal[k]);
+      if (n == 0) continue;
+      const unsigned long long p0 = prefix + S.warp_cnt[k][wid];
+      const uint32_t words = n * out_cols;
+      for (uint32_t base = 0; base < words; base += 32) {
+        const uint32_t w = base + lane;
+        const uint32_t q = (w < words ? w : words - 1) / out_cols;  // q-th kept candidate of the slice
+        const uint32_t c = w - q * out_cols;
+        const uint32_t src = __fns(bal[k], 0, q + 1);  // lane holding it
+        const unsigned long long r = __shfl_sync(0xffffffffu, rv[k], src);
+        const uint32_t y = __shfl_sync(0xffffffffu, yv[k], src);
+        if (w < words && p0 + q < out_cap)
+          out[(p0 + q) * out_cols + c] = (c < cols) ? __ldg(in + (row_begin + r) * cols + c) : y;
+      }
+    }
+  }
+  // the last block to finish moves the ticket counter to the end of the
+  // range the host reserved, so the next launch's base is exact
   __syncthreads();
-  const uint32_t cut = S.cut;
-  if (threadIdx.x == 0 && cut < nrows) {
-    atomicMin(&res->cut_row, first + cut);
-    atomicMin(&res->cut_pos, prefix + S.off[cut]);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long done = atomicAdd(&st->blocks_done, 1ULL);
+    if (done == gridDim.x - 1) atomicExch(lb.ticket, lb.base + reserved);
   }
-  // pass 2: write the rows that fit
-  for (uint32_t i = 0; i < kExpRowsPerWarp; ++i) {
-    const uint32_t rl = wid * kExpRowsPerWarp + i;
-    if (rl >= nrows || rl >= cut) break;
-    const unsigned long long pos = prefix + S.off[rl];
-    if (S.cnt[rl] == 0 || pos >= out_cap) continue;
-    unsigned long long dl;
-    expand_row(S, wid, in, cols, first + rl, nb, true, out, pos, out_cap, &dl);
-  }
-  if (threadIdx.x == 0 && tile == ntiles - 1) res->total = prefix + total;
 }
 
 __global__ void k_gather_u64(const unsigned long long* __restrict__ src, const unsigned long long* __restrict__ idx,
@@ -243,14 +307,10 @@ void launch_gather_u64(Workspace& ws, const unsigned long long* src, const unsig
   GPSM_LAUNCHED();
 }
 
-void launch_expand(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
-                   const BackNbr* d_back, uint32_t nb, uint32_t* out, uint64_t out_cap, bool partial,
-                   ExpandResult* d_res, uint64_t nbrs_total) {
-  if (row_end <= row_begin) return;
-  const uint64_t tiles = (row_end - row_begin + kExpTile - 1) / kExpTile;
+static Lookback next_lb(Workspace& ws, uint64_t tiles) {
   if (tiles > ws.scan.max_tiles) {
-    set_last_error("expand: too many tiles for the scan state");
-    throw CudaError{cudaErrorInvalidValue, "expand tiles"};
+    set_last_error("join step: too many tiles for the scan state");
+    throw CudaError{cudaErrorInvalidValue, "join tiles"};
   }
   Lookback lb;
   lb.ticket = ws.scan.d_ticket;
@@ -261,12 +321,34 @@ void launch_expand(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t
   lb.base = base;
   lb.epoch = ep;
   lb.flags = ws.d_flags;
-  k_expand<<<(uint32_t)tiles, kExpBlock, 0, ws.stream>>>(in, in_cols, row_begin, row_end, d_back, nb, out, out_cap,
-                                                         partial ? 1u : 0u, d_res, lb,
-                                                         (unsigned long long)nbrs_total);
-  GPSM_LAUNCHED();
+  return lb;
 }
 
-uint64_t expand_tile_rows() { return kExpTile; }
+uint64_t join_rows_per_locate_tile() { return kLocBlock; }
+
+void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
+                      const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st) {
+  const uint64_t nrows = row_end - row_begin;
+  if (nrows == 0) return;
+  if (nrows > js.rows || nrows * nb > js.rng_entries) {
+    set_last_error("join step: more rows than the step scratch holds");
+    throw CudaError{cudaErrorInvalidValue, "join rows"};
+  }
+  const uint64_t ltiles = (nrows + kLocBlock - 1) / kLocBlock;
+  Lookback lb1 = next_lb(ws, ltiles);
+  k_locate<<<(uint32_t)ltiles, kLocBlock, 0, ws.stream>>>(in, in_cols, row_begin, nrows, d_back, nb, nbrs_total,
+                                                          budget, js.drv, js.rng, js.coff, d_st, lb1);
+  GPSM_LAUNCHED();
+  // k_extend is persistent: blocks take tiles by ticket until the admitted
+  // candidates run out, then each takes one terminating ticket. The host
+  // reserves the worst case; the kernel's last block moves the counter to
+  // the end of the reservation.
+  const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + kExtGrid;
+  Lookback lb2 = next_lb(ws, reserved);
+  k_extend<<<kExtGrid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
+                                                  js.coff, out, out_cap, d_st, lb2, (unsigned long long)reserved);
+  GPSM_LAUNCHED();
+}
 
 }  // namespace gpsm

@@ -150,7 +150,16 @@ def sum_over_ranks(pg, x):
     return float(t.item())
 
 
-def load_workload(name, rank, count=None):
+def load_workload(name, rank, count=None, first=0, take=None):
+    wl = _load_workload(name, rank, count)
+    if first or take:
+        from gpsm_b200 import workloads as W
+        qs = wl.queries[first:first + take] if take else wl.queries[first:]
+        wl = W.Workload(wl.name, wl.graph, qs)
+    return wl
+
+
+def _load_workload(name, rank, count=None):
     from gpsm_b200 import workloads as W
     wl = W.workload(name, count=count)
     if rank > 0:  # every rank its own batch of the same shape (replicas, weak scaling)
@@ -175,7 +184,7 @@ def run_ours(args):
     rank, world, local, pg = dist_setup(args.gpus)
     import gpsm_b200 as G
     G.init(local)
-    wl = load_workload(args.workload, rank)
+    wl = load_workload(args.workload, rank, first=args.first, take=args.count)
     dg = G.DeviceGraph(wl.graph)
     packed = G.pack_queries(wl.queries)
     nq = len(wl.queries)
@@ -271,7 +280,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    wl = load_workload(args.workload, 0)
+    wl = load_workload(args.workload, 0, first=args.first, take=args.count)
     for _ in range(args.warmup):
         pass  # the CPU port has no warm-up state worth priming beyond the first sample
     rates, dones = [], []
@@ -317,6 +326,8 @@ def main():
     ap.add_argument("--order", default="plain", choices=["plain"])
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--first", type=int, default=0, help="first query of the batch (profiling subsets)")
+    ap.add_argument("--count", type=int, default=0, help="queries from --first (0 = all)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -59,22 +59,35 @@ SIGNATURES = {
     "gpsm_debug_filter": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_match_batch": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_flush_l2": (C.c_int, [vp, u64]),
+    "gpsm_select_vertices": (C.c_int, [vp, vp, vp, u32, u32, u32, vp, vp]),
+    "gpsm_last_levels": (C.c_int, [vp, u32, vp, vp, vp]),
+    "gpsm_model_params": (C.c_int, []),
+    "gpsm_model_create": (C.c_int, [C.c_int, u64, vp]),
+    "gpsm_model_destroy": (C.c_int, [vp]),
+    "gpsm_model_set": (C.c_int, [vp, vp]),
+    "gpsm_model_get": (C.c_int, [vp, vp]),
+    "gpsm_model_train": (C.c_int, [vp, vp, vp, u32, u32, u32, C.c_float, u64, vp]),
+    "gpsm_model_grad": (C.c_int, [vp, vp, vp, u32, vp, vp]),
+    "gpsm_model_predict": (C.c_int, [vp, vp, u32, vp]),
+    "gpsm_order_features": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
 }
 
-GPSM_ORDER_PLAIN, GPSM_ORDER_GIVEN = 0, 1
+GPSM_ORDER_PLAIN, GPSM_ORDER_GIVEN, GPSM_ORDER_LEARNED = 0, 1, 2
 GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE = 1, 2
 
 
 class MatchOpts(C.Structure):
     _fields_ = [("cap", u64), ("order_mode", i32), ("pad", i32), ("order", vp),
-                ("level_bytes", u64), ("result_rows", u64), ("flags", u32), ("pad2", u32)]
+                ("level_bytes", u64), ("result_rows", u64), ("flags", u32), ("pad2", u32),
+                ("model", vp), ("memory_budget", u64), ("work_cap", u64)]
 
 
 class MatchInfo(C.Structure):
     _fields_ = [("rows", u64), ("cols", u32), ("capped", i32), ("empty_filter", i32), ("pad", i32),
                 ("device_ms", f64), ("filter_ms", f64), ("join_ms", f64),
                 ("expand_launches", u64), ("filter_launches", u64), ("alg_bytes_join", u64),
-                ("expand_ms", f64)]
+                ("expand_ms", f64), ("plan_ms", f64), ("predicted_work", f64), ("predicted_peak", f64),
+                ("order_fallback", i32), ("aborted", i32)]
 
 
 class BatchInfo(C.Structure):

@@ -12,11 +12,16 @@
 #include <new>
 
 #include "engine.h"
+#include "learned.h"
 
 using namespace gpsm;
 
 struct gpsm_graph_s {
   DeviceGraph* g;
+};
+
+struct gpsm_model_s {
+  Model* m;
 };
 
 struct gpsm_engine_s {
@@ -77,6 +82,12 @@ MatchOptions to_options(const gpsm_match_opts* o) {
   if (o->result_rows) m.result_rows = o->result_rows;
   m.keep_on_device = (o->flags & GPSM_F_KEEP_ON_DEVICE) != 0;
   m.collect_rows = (o->flags & GPSM_F_COUNT_ONLY) == 0;
+  if (o->order_mode == GPSM_ORDER_LEARNED) {
+    m.order_mode = ORDER_LEARNED;
+    m.model = o->model ? o->model->m : nullptr;
+  }
+  m.memory_budget = o->memory_budget;
+  m.work_cap = o->work_cap;
   return m;
 }
 
@@ -94,6 +105,11 @@ void fill_info(const MatchResult& R, gpsm_match_info* info) {
   info->filter_launches = R.stats.filter_launches;
   info->alg_bytes_join = R.stats.alg_bytes_join;
   info->expand_ms = R.stats.expand_ms;
+  info->plan_ms = R.stats.plan_ms;
+  info->predicted_work = R.stats.predicted_work;
+  info->predicted_peak = R.stats.predicted_peak;
+  info->order_fallback = R.stats.order_fallback ? 1 : 0;
+  info->aborted = R.stats.aborted ? 1 : 0;
 }
 
 }  // namespace
@@ -281,6 +297,115 @@ int gpsm_match(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t q
 
 void gpsm_free(void* p) { free(p); }
 
+int gpsm_last_levels(gpsm_engine_t eng, uint32_t n, uint64_t* level_in, uint64_t* level_cands, uint64_t* level_out) {
+  gpsm_engine_s* e = engine_or_default(eng);
+  if (!e) return GPSM_ERR_STATE;
+  std::lock_guard<std::mutex> lk(e->mu);
+  const MatchStats& st = e->last.stats;
+  for (uint32_t w = 0; w <= n; ++w) {
+    if (level_in) level_in[w] = w < st.level_in.size() ? st.level_in[w] : 0;
+    if (level_cands) level_cands[w] = w < st.level_cands.size() ? st.level_cands[w] : 0;
+    if (level_out) level_out[w] = w < st.level_rows.size() ? st.level_rows[w] : 0;
+  }
+  return GPSM_OK;
+}
+
+int gpsm_model_params(void) { return kParams; }
+
+int gpsm_model_create(int dev, uint64_t seed, gpsm_model_t* out) {
+  if (!out) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    gpsm_model_s* h = new gpsm_model_s();
+    h->m = model_create(dev, seed);
+    *out = h;
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_destroy(gpsm_model_t m) {
+  if (!m) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    model_free(m->m);
+    delete m;
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_set(gpsm_model_t m, const float* params) {
+  if (!m || !params) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    model_set(m->m, params);
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_get(gpsm_model_t m, float* params) {
+  if (!m || !params) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    model_get(m->m, params);
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_train(gpsm_model_t m, const float* x, const float* y, uint32_t n, uint32_t epochs, uint32_t batch,
+                     float lr, uint64_t seed, float* loss) {
+  if (!m || !x || !y || n == 0) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    float l = model_train(m->m, x, y, n, epochs, batch, lr, seed);
+    if (loss) *loss = l;
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_grad(gpsm_model_t m, const float* x, const float* y, uint32_t n, float* grad, float* loss) {
+  if (!m || !x || !y || !grad || n == 0) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    float l = model_grad(m->m, x, y, n, grad);
+    if (loss) *loss = l;
+    return GPSM_OK;
+  });
+}
+
+int gpsm_model_predict(gpsm_model_t m, const float* x, uint32_t n, float* y) {
+  if (!m || !x || !y) return GPSM_ERR_INVALID;
+  if (n == 0) return GPSM_OK;
+  return guarded([&]() -> int {
+    model_predict(m->m, x, n, y);
+    return GPSM_OK;
+  });
+}
+
+int gpsm_order_features(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm, const uint32_t* q_edges,
+                        const uint32_t* cand_count, const uint64_t* size_fwd, const uint64_t* size_rev,
+                        const int32_t* pos2id, float* out) {
+  if (!g || !cand_count || !pos2id || !out || (qm && (!size_fwd || !size_rev))) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    QueryPlan Q;
+    std::string err;
+    int rc = plan_query(*g->g, qn, q_labels, qm, q_edges, Q, err);
+    if (rc != GPSM_OK) {
+      set_last_error(err);
+      return rc;
+    }
+    if (qn > (uint32_t)kMaxPlanQ) {
+      set_last_error("query too large for the planner");
+      return GPSM_ERR_INVALID;
+    }
+    std::vector<int32_t> ord(pos2id, pos2id + qn);
+    if (!valid_order(Q, ord)) {
+      set_last_error("order is not a connected permutation");
+      return GPSM_ERR_INVALID;
+    }
+    std::vector<uint32_t> cand(cand_count, cand_count + qn);
+    std::vector<uint64_t> sf(size_fwd, size_fwd + qm), sr(size_rev, size_rev + qm);
+    std::unique_ptr<PlanQuery> PQ(new PlanQuery());
+    std::unique_ptr<PlanEdges> PE(new PlanEdges());
+    build_plan_inputs(*g->g, Q, cand, sf, sr, *PQ, *PE);
+    order_features(*PQ, *PE, ord, out);
+    return GPSM_OK;
+  });
+}
+
 // Throughput entry point: matches nq queries back to back on one engine.
 // Rows are produced in device memory and overwritten by the next query
 // (GPSM_F_KEEP_ON_DEVICE is implied); counts, cap flags and per-query device
@@ -336,6 +461,39 @@ int gpsm_match_batch(gpsm_engine_t eng, gpsm_graph_t g, uint32_t nq, const uint3
     GPSM_CUDA(cudaEventElapsedTime(&ms, ws.evb0, ws.evb1));
     bi.device_ms = ms;
     if (info) *info = bi;
+    return GPSM_OK;
+  });
+}
+
+// Vertices of a device-resident graph with `label` and degree >= min_degree,
+// ascending, as the reference's check_kernel + kernel_collect compute them
+// (match/Match.cu:431-526). d_labels[n], d_offsets[n+1]: device arrays;
+// d_out: device, room for n ids; d_count: device, one u32. Scratch (the
+// selection bitmap and the scan state) comes from the engine's workspace.
+// Runs on the engine's stream and returns after it finishes.
+int gpsm_select_vertices(gpsm_engine_t eng, const uint32_t* d_labels, const uint32_t* d_offsets, uint32_t n,
+                         uint32_t label, uint32_t min_degree, uint32_t* d_out, uint32_t* d_count) {
+  gpsm_engine_s* e = engine_or_default(eng);
+  if (!e) {
+    set_last_error("gpsm_init was not called");
+    return GPSM_ERR_STATE;
+  }
+  if (!d_labels || !d_offsets || !d_out || !d_count || n == 0) {
+    set_last_error("gpsm_select_vertices: null array or n == 0");
+    return GPSM_ERR_INVALID;
+  }
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(e->mu);
+    Workspace& ws = *e->ws;
+    ws.arena.reset();
+    uint32_t* bm = (uint32_t*)ws.arena.alloc((size_t)select_words(n) * 4);
+    if (!bm) {
+      set_last_error("gpsm_select_vertices: workspace too small");
+      return GPSM_ERR_NOMEM;
+    }
+    GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, sizeof(uint32_t), ws.stream));
+    select_vertices(ws, d_labels, d_offsets, n, label, min_degree, bm, d_out, d_count);
+    GPSM_CUDA(cudaStreamSynchronize(ws.stream));
     return GPSM_OK;
   });
 }

@@ -15,8 +15,11 @@
 //     query after exactly `cap` rows (the first `cap` in row order).
 #include "engine.h"
 
+#include "learned.h"
+
 #include <algorithm>
 #include <chrono>
+#include <memory>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -194,6 +197,45 @@ std::vector<int32_t> plain_order(const QueryPlan& Q, const std::vector<uint64_t>
   return pos2id;
 }
 
+void build_plan_inputs(const DeviceGraph& g, const QueryPlan& Q, const std::vector<uint32_t>& cand,
+                       const std::vector<uint64_t>& size_fwd, const std::vector<uint64_t>& size_rev, PlanQuery& PQ,
+                       PlanEdges& PE) {
+  memset(&PQ, 0, sizeof(PQ));
+  PQ.n = Q.n;
+  for (uint32_t u = 0; u < Q.n; ++u) {
+    for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) {
+      const uint32_t w = Q.rcol[k];
+      PQ.adj[u][w >> 6] |= 1ULL << (w & 63);
+    }
+    PQ.label[u] = Q.lab[u];
+    PQ.qdeg[u] = Q.deg(u);
+    PQ.log_cand[u] = std::log2(1.0f + (float)cand[u]);
+    uint32_t b, e;
+    g.label_range(Q.lab[u], Q.deg(u), &b, &e);
+    PQ.log_labdeg[u] = std::log2(1.0f + (float)(e - b));
+    PQ.log_label[u] = std::log2(1.0f + (float)g.label_count(Q.lab[u]));
+  }
+  for (size_t i = 0; i < (size_t)kMaxPlanQ * kMaxPlanQ; ++i) PE.log_size[i] = PE.log_avg[i] = 0.f;
+  for (uint32_t e = 0; e < Q.m; ++e) {
+    const uint32_t a = Q.efrom[e], b = Q.eto[e];
+    const float sf = (float)size_fwd[e], sr = (float)size_rev[e];
+    PE.log_size[a * kMaxPlanQ + b] = std::log2(1.f + sf);
+    PE.log_size[b * kMaxPlanQ + a] = std::log2(1.f + sr);
+    PE.log_avg[a * kMaxPlanQ + b] = std::log2(1.f + sf / std::max(1.f, (float)cand[a]));
+    PE.log_avg[b * kMaxPlanQ + a] = std::log2(1.f + sr / std::max(1.f, (float)cand[b]));
+  }
+}
+
+void order_features(const PlanQuery& PQ, const PlanEdges& PE, const std::vector<int32_t>& pos2id, float* out) {
+  uint64_t P[2] = {0, 0};
+  P[pos2id[0] >> 6] |= 1ULL << (pos2id[0] & 63);
+  for (uint32_t k = 1; k < pos2id.size(); ++k) {
+    const uint32_t v = (uint32_t)pos2id[k];
+    step_features(PQ, PE, P, k, v, out + (size_t)(k - 1) * kFeat);
+    P[v >> 6] |= 1ULL << (v & 63);
+  }
+}
+
 bool valid_order(const QueryPlan& Q, const std::vector<int32_t>& pos2id) {
   if (pos2id.size() != Q.n) return false;
   std::vector<uint8_t> seen(Q.n, 0);
@@ -237,6 +279,81 @@ struct Level {
 };
 
 }  // namespace
+
+void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const PlanEdges* d_e, const uint32_t* d_starts,
+                 uint32_t nstarts, void* d_out);
+size_t plan_out_bytes();
+
+// Learned order: greedy MLP plans from up to 8 start vertices on the device;
+// the plan with the smallest predicted work wins. Returns {} (plain order)
+// when its predicted peak table exceeds the memory budget.
+static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q,
+                                          const std::vector<uint32_t>& cnt, const std::vector<uint64_t>& size_fwd,
+                                          const std::vector<uint64_t>& size_rev, const MatchOptions& opt,
+                                          MatchStats& st) {
+  static thread_local std::unique_ptr<PlanQuery> PQ(new PlanQuery());
+  static thread_local std::unique_ptr<PlanEdges> PE(new PlanEdges());
+  build_plan_inputs(g, Q, cnt, size_fwd, size_rev, *PQ, *PE);
+  // starts: endpoints of the two smallest forward candidate-edge sets, then
+  // the vertices with the fewest candidates
+  std::vector<uint32_t> starts;
+  auto add = [&](uint32_t v) {
+    if (starts.size() < 8 && std::find(starts.begin(), starts.end(), v) == starts.end()) starts.push_back(v);
+  };
+  std::vector<uint32_t> eidx(Q.m);
+  for (uint32_t e = 0; e < Q.m; ++e) eidx[e] = e;
+  std::sort(eidx.begin(), eidx.end(), [&](uint32_t a, uint32_t b) {
+    return size_fwd[a] != size_fwd[b] ? size_fwd[a] < size_fwd[b] : a < b;
+  });
+  for (uint32_t i = 0; i < std::min<uint32_t>(2, Q.m); ++i) {
+    add(Q.efrom[eidx[i]]);
+    add(Q.eto[eidx[i]]);
+  }
+  std::vector<uint32_t> vidx(Q.n);
+  for (uint32_t u = 0; u < Q.n; ++u) vidx[u] = u;
+  std::sort(vidx.begin(), vidx.end(), [&](uint32_t a, uint32_t b) { return cnt[a] != cnt[b] ? cnt[a] < cnt[b] : a < b; });
+  for (uint32_t u : vidx) add(u);
+  const size_t mark = ws.arena.used;
+  PlanQuery* d_q = arena_alloc<PlanQuery>(ws, 1);
+  PlanEdges* d_e = arena_alloc<PlanEdges>(ws, 1);
+  uint32_t* d_st = arena_alloc<uint32_t>(ws, 8);
+  char* d_out = arena_alloc<char>(ws, plan_out_bytes() * 8);
+  cudaStream_t s = ws.stream;
+  GPSM_CUDA(cudaMemcpyAsync(d_q, PQ.get(), sizeof(PlanQuery), cudaMemcpyHostToDevice, s));
+  // only the rows of the n query vertices matter; copy the whole table for simplicity
+  GPSM_CUDA(cudaMemcpyAsync(d_e, PE.get(), sizeof(PlanEdges), cudaMemcpyHostToDevice, s));
+  GPSM_CUDA(cudaMemcpyAsync(d_st, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
+  launch_plan(s, opt.model, d_q, d_e, d_st, (uint32_t)starts.size(), d_out);
+  std::vector<char> hout(plan_out_bytes() * starts.size());
+  GPSM_CUDA(cudaMemcpyAsync(hout.data(), d_out, hout.size(), cudaMemcpyDeviceToHost, s));
+  GPSM_CUDA(cudaStreamSynchronize(s));
+  ws.arena.used = mark;  // planner scratch is not needed by the joins
+  const size_t ob = plan_out_bytes();
+  int best = -1;
+  float best_work = 0.f, best_peak = 0.f;
+  for (size_t i = 0; i < starts.size(); ++i) {
+    const int32_t* order = reinterpret_cast<const int32_t*>(hout.data() + i * ob);
+    const float work = *reinterpret_cast<const float*>(hout.data() + i * ob + kMaxPlanQ * 4);
+    const float peak = *reinterpret_cast<const float*>(hout.data() + i * ob + kMaxPlanQ * 4 + 4);
+    std::vector<int32_t> ord(order, order + Q.n);
+    if (!valid_order(Q, ord)) continue;
+    if (best < 0 || work < best_work) {
+      best = (int)i;
+      best_work = work;
+      best_peak = peak;
+    }
+  }
+  st.predicted_work = best_work;
+  st.predicted_peak = best_peak;
+  if (best < 0) return {};
+  const uint64_t budget = opt.memory_budget ? opt.memory_budget : ws.arena.size;
+  if ((double)best_peak > (double)budget) {
+    st.order_fallback = true;
+    return {};
+  }
+  const int32_t* order = reinterpret_cast<const int32_t*>(hout.data() + (size_t)best * ob);
+  return std::vector<int32_t>(order, order + Q.n);
+}
 
 int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R) {
   R = MatchResult();
@@ -439,6 +556,15 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       return GPSM_ERR_INVALID;
     }
     pos2id = opt.given_order;
+  } else if (opt.order_mode == ORDER_LEARNED && qn > 2 && qn <= (uint32_t)kMaxPlanQ) {
+    if (!opt.model) {
+      set_last_error("learned order requested without a model");
+      return GPSM_ERR_INVALID;
+    }
+    const auto tp0 = std::chrono::steady_clock::now();
+    pos2id = learned_order(ws, g, Q, cnt, R.stats.size_fwd, R.stats.size_rev, opt, R.stats);
+    if (pos2id.empty()) pos2id = plain_order(Q, R.stats.size_fwd, g.nnz);
+    R.stats.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count();
   } else {
     pos2id = plain_order(Q, R.stats.size_fwd, g.nnz);
   }
@@ -491,6 +617,9 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
   R.stats.level_rows.assign(qn + 1, 0);
+  R.stats.level_in.assign(qn + 1, 0);
+  R.stats.level_cands.assign(qn + 1, 0);
+  uint64_t cands_total = 0;
   const uint64_t cap = opt.cap;
   // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
   std::vector<Level> L(qn + 1);
@@ -622,6 +751,17 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     A.next = rb + admitted;
     alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
     R.stats.level_rows[lv + 1] += written;
+    R.stats.level_in[lv] += admitted;
+    R.stats.level_cands[lv] += cands;
+    cands_total += cands;
+    if (opt.work_cap && cands_total >= opt.work_cap) {
+      R.stats.aborted = true;
+      if (final_level) {
+        res_used += written;
+        emitted += written;
+      }
+      break;
+    }
     if (final_level) {
       res_used += written;
       emitted += written;

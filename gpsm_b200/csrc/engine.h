@@ -38,7 +38,17 @@ std::vector<int32_t> plain_order(const QueryPlan& Q, const std::vector<uint64_t>
 // has an earlier neighbour.
 bool valid_order(const QueryPlan& Q, const std::vector<int32_t>& pos2id);
 
-enum OrderMode : int { ORDER_PLAIN = 0, ORDER_GIVEN = 1 };
+enum OrderMode : int { ORDER_PLAIN = 0, ORDER_GIVEN = 1, ORDER_LEARNED = 2 };
+
+struct Model;  // learned.cu
+Model* model_create(int device, uint64_t seed);
+void model_free(Model* M);
+void model_set(Model* M, const float* w);
+void model_get(Model* M, float* w);
+float model_grad(Model* M, const float* x, const float* y, uint32_t n, float* grad);
+float model_train(Model* M, const float* x, const float* y, uint32_t n, uint32_t epochs, uint32_t batch, float lr,
+                  uint64_t seed);
+void model_predict(Model* M, const float* x, uint32_t n, float* y);
 
 struct MatchOptions {
   uint64_t cap = ~0ULL;            // embedding cap (rows after which the query stops)
@@ -51,18 +61,27 @@ struct MatchOptions {
   bool keep_on_device = false;          // never flush: fail with GPSM_ERR_BUDGET instead
   bool collect_rows = true;             // false: count only (result rows are discarded)
   bool filter_only = false;             // stop after the join order (debug entry points)
+  Model* model = nullptr;               // ORDER_LEARNED
+  uint64_t memory_budget = 0;           // bytes; predicted peak above it -> plain order (0 = arena size)
+  uint64_t work_cap = 0;                // candidates the joins may scan before stopping (0 = none)
 };
 
 struct MatchStats {
   std::vector<uint32_t> cand_count;      // final |C(u)|
   std::vector<uint64_t> size_fwd, size_rev;  // candidate-edge totals per edge id
   std::vector<uint64_t> level_rows;      // rows produced at each table width 1..n
+  std::vector<uint64_t> level_in;        // rows of width w extended (admitted) by join steps
+  std::vector<uint64_t> level_cands;     // candidates scanned when extending width w
   uint64_t expand_launches = 0;
   uint64_t filter_launches = 0;
   double device_ms = 0;
   double filter_ms = 0, join_ms = 0;
   uint64_t alg_bytes_join = 0;  // algorithmic bytes of the join phase
   double expand_ms = 0;         // summed device time of the join launches
+  double plan_ms = 0;           // learned-order planning (host wall time incl. the planner kernel)
+  double predicted_work = 0, predicted_peak = 0;
+  bool order_fallback = false;  // learned order rejected by the memory budget
+  bool aborted = false;         // work cap reached
   uint64_t alg_bytes_filter = 0;
 };
 
@@ -79,5 +98,19 @@ struct MatchResult {
 };
 
 int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R);
+
+struct PlanQuery;
+struct PlanEdges;
+// Planner inputs from the filter statistics (learned.h).
+void build_plan_inputs(const DeviceGraph& g, const QueryPlan& Q, const std::vector<uint32_t>& cand,
+                       const std::vector<uint64_t>& size_fwd, const std::vector<uint64_t>& size_rev, PlanQuery& PQ,
+                       PlanEdges& PE);
+// Features of every step of the order pos2id ((n-1) x kFeat floats).
+void order_features(const PlanQuery& PQ, const PlanEdges& PE, const std::vector<int32_t>& pos2id, float* out);
+
+// vertices with `label` and degree >= min_degree, ascending (select.cu)
+uint32_t select_words(uint32_t n);
+void select_vertices(Workspace& ws, const uint32_t* d_labels, const uint32_t* d_offsets, uint32_t n, uint32_t label,
+                     uint32_t min_degree, uint32_t* bm, uint32_t* d_out, uint32_t* d_count);
 
 }  // namespace gpsm

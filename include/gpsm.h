@@ -85,6 +85,9 @@ int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_de
 
 #define GPSM_ORDER_PLAIN 0 /* the reference's join order (match/Match.cu:1599-1694) */
 #define GPSM_ORDER_GIVEN 1 /* opts.order gives the table columns (pos -> query vertex) */
+#define GPSM_ORDER_LEARNED 2 /* opts.model chooses the order (plain order beyond the memory budget) */
+
+typedef struct gpsm_model_s* gpsm_model_t; /* learned join-order model (MLP on one device) */
 
 #define GPSM_F_COUNT_ONLY 1u      /* do not return rows (count and statistics only) */
 #define GPSM_F_KEEP_ON_DEVICE 2u  /* rows stay in device memory; never spill to host */
@@ -98,6 +101,9 @@ typedef struct gpsm_match_opts {
   uint64_t result_rows;  /* device result buffer rows; 0 = 4 Mi */
   uint32_t flags;        /* GPSM_F_* */
   uint32_t pad2;
+  gpsm_model_t model;    /* GPSM_ORDER_LEARNED */
+  uint64_t memory_budget; /* bytes: predicted peak table above it -> plain order (0 = workspace size) */
+  uint64_t work_cap;     /* candidates the joins may scan before the query stops (0 = none) */
 } gpsm_match_opts;
 
 typedef struct gpsm_match_info {
@@ -113,6 +119,11 @@ typedef struct gpsm_match_info {
   uint64_t filter_launches;
   uint64_t alg_bytes_join;   /* algorithmic bytes of the joins (roofline numerator) */
   double expand_ms;          /* summed device time of the join launches */
+  double plan_ms;            /* learned-order planning */
+  double predicted_work;     /* learned order: predicted sum of table sizes */
+  double predicted_peak;     /* learned order: predicted peak table bytes */
+  int32_t order_fallback;    /* 1: learned order over the memory budget, plain order used */
+  int32_t aborted;           /* 1: work_cap stopped the joins (rows are a prefix) */
 } gpsm_match_info;
 
 typedef struct gpsm_batch_info {
@@ -153,8 +164,46 @@ int gpsm_match_batch(gpsm_engine_t e, gpsm_graph_t g, uint32_t nq, const uint32_
                      const uint32_t* q_labels, const uint64_t* q_eoff, const uint32_t* q_edges,
                      const gpsm_match_opts* opts, const int32_t* orders, uint64_t* counts,
                      int32_t* capped, double* query_ms, gpsm_batch_info* info);
+/* Vertices with `label` and degree >= min_degree, ascending, on device
+ * arrays (d_labels[n], d_offsets[n+1]); d_out (device) must hold n ids,
+ * d_count (device) gets the count. Replaces check_kernel + kernel_collect
+ * (match/Match.cu:431-526). Scratch comes from the engine's workspace
+ * (e = NULL: the default engine); returns after the work finishes. */
+int gpsm_select_vertices(gpsm_engine_t e, const uint32_t* d_labels, const uint32_t* d_offsets,
+                         uint32_t n, uint32_t label, uint32_t min_degree, uint32_t* d_out,
+                         uint32_t* d_count);
 /* Writes `bytes` of device memory on the engine's stream (an L2 flush). */
 int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
+
+/* Per-width join statistics of the engine's last gpsm_match_ex/
+ * gpsm_engine_match call (n+1 entries each, index = table width):
+ * rows extended, candidates scanned, rows produced. */
+int gpsm_last_levels(gpsm_engine_t e, uint32_t n, uint64_t* level_in, uint64_t* level_cands,
+                     uint64_t* level_out);
+
+/* ---- learned join order (no counterpart in the reference) -------------- */
+/* 16 -> 64 -> 64 -> 1 MLP, BF16 weights, FP32 accumulation and masters.
+ * It predicts log2(rows out / rows in) of the join step that adds a query
+ * vertex to the placed set, from 16 features of the query and the filter
+ * statistics (gpsm_order_features). */
+int gpsm_model_params(void);
+int gpsm_model_create(int dev, uint64_t seed, gpsm_model_t* out);
+int gpsm_model_destroy(gpsm_model_t m);
+int gpsm_model_set(gpsm_model_t m, const float* params);
+int gpsm_model_get(gpsm_model_t m, float* params);
+/* Adam on minibatches of (x[n][16], y[n]) on the GPU; *loss = last epoch. */
+int gpsm_model_train(gpsm_model_t m, const float* x, const float* y, uint32_t n, uint32_t epochs,
+                     uint32_t batch, float lr, uint64_t seed, float* loss);
+/* Gradient of the mean squared error over all n samples, no update. */
+int gpsm_model_grad(gpsm_model_t m, const float* x, const float* y, uint32_t n, float* grad,
+                    float* loss);
+int gpsm_model_predict(gpsm_model_t m, const float* x, uint32_t n, float* y);
+/* Features of every step of a vertex order (pos2id) for one query, from the
+ * filter statistics gpsm_debug_filter returns: out[(qn-1)*16]. */
+int gpsm_order_features(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
+                        const uint32_t* q_edges, const uint32_t* cand_count,
+                        const uint64_t* size_fwd, const uint64_t* size_rev,
+                        const int32_t* pos2id, float* out);
 
 /* Filter-stage results for comparison with the reference restatement:
  * final |C(u)|, candidate-edge totals per edge id (forward = from->to with

@@ -178,3 +178,25 @@ def test_rmat20_filter_and_capped_rows(gpu, rmat20):
             continue  # oracle stopped on its work bound, not on the cap
         assert out.count == ref_cnt
         assert np.array_equal(out.rows, ref_rows)
+
+
+def test_select_vertices_matches_label_degree_filter(gpu, lib):
+    """check_kernel + kernel_collect as a primitive: ids with the label and
+    degree >= d, ascending (match/Match.cu:431-526)."""
+    import ctypes as C
+    import torch
+    g = W.rmat_graph(16, 200000, 8, 1.0, seed=11)
+    lab = torch.from_numpy(g.labels.astype(np.int32)).cuda()
+    off = torch.from_numpy(g.offsets.astype(np.int64).astype(np.int32)).cuda()
+    out = torch.zeros(g.n, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    deg = np.diff(g.offsets.astype(np.int64))
+    for label, d in [(1, 0), (2, 3), (5, 20), (99, 0)]:
+        rc = lib.gpsm_select_vertices(None, C.c_void_p(lab.data_ptr()), C.c_void_p(off.data_ptr()), g.n, label, d,
+                                      C.c_void_p(out.data_ptr()), C.c_void_p(cnt.data_ptr()))
+        assert rc == 0
+        torch.cuda.synchronize()
+        want = np.flatnonzero((g.labels == label) & (deg >= d))
+        k = int(cnt.item())
+        assert k == len(want)
+        assert np.array_equal(out[:k].cpu().numpy().astype(np.int64), want)

@@ -60,6 +60,7 @@ SIGNATURES = {
     "gpsm_match_batch": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_flush_l2": (C.c_int, [vp, u64]),
     "gpsm_select_vertices": (C.c_int, [vp, vp, vp, u32, u32, u32, vp, vp]),
+    "gpsm_select_vertices_static": (C.c_int, [vp, vp, u32, u32, u32, vp, vp, vp]),
     "gpsm_last_levels": (C.c_int, [vp, u32, vp, vp, vp]),
     "gpsm_model_params": (C.c_int, []),
     "gpsm_model_create": (C.c_int, [C.c_int, u64, vp]),

@@ -172,6 +172,19 @@ int gpsm_match_batch(gpsm_engine_t e, gpsm_graph_t g, uint32_t nq, const uint32_
 int gpsm_select_vertices(gpsm_engine_t e, const uint32_t* d_labels, const uint32_t* d_offsets,
                          uint32_t n, uint32_t label, uint32_t min_degree, uint32_t* d_out,
                          uint32_t* d_count);
+/* gpsm_select_vertices for callers that cannot allocate device memory (a
+ * host that owns every allocation, such as a framework pool or a plugin host,
+ * or a caller that cannot pay for cudaMalloc at call time). No counterpart in
+ * the reference. It allocates nothing: its scratch is a fixed array of about
+ * 513 KiB compiled into the library (held on every GPU that loads it), so n
+ * is limited to 4194304 vertices (larger n: GPSM_ERR_BUDGET). Runs on
+ * `stream` (a cudaStream_t, NULL = default stream) of the current device and
+ * returns after it finishes. The first call on a device looks up the array's
+ * device address; make it before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race. Needs no gpsm_init. */
+int gpsm_select_vertices_static(const uint32_t* d_labels, const uint32_t* d_offsets, uint32_t n,
+                                uint32_t label, uint32_t min_degree, uint32_t* d_out,
+                                uint32_t* d_count, void* stream);
 /* Writes `bytes` of device memory on the engine's stream (an L2 flush). */
 int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
 

@@ -1,17 +1,20 @@
 """Throughput benchmark of the subgraph-matching path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rmat20] [--order plain] [--cap 10000000]
+                    [--workload rmat20] [--order learned|plain] [--slots 4] [--cap 10000000]
 
 A step is one pass of the path over one batch of queries against the
 device-resident data graph (default: the R-MAT 2^20 workload, 100 induced
 random-walk queries of 12 vertices, 10^7-embedding cap per query).
 
 value: queries/s over the K timed steps with the graph and the query batch
-already resident (device events on the engine stream, L2 flushed between
-steps). e2e: the same metric through the C ABI entry point a caller uses
-(gpsm_match_ex per query) with host buffers: query upload and the copy of
-every embedding row back to host memory are inside the timed region.
+already resident, with the learned join order and `--slots` engine slots
+(continuous batching); device time from events on the slots' streams, L2
+flushed between steps. plain_order: one step of the reference's join order
+on one slot (the plain GpSM-order GPU path), for the learned+batched ratio.
+e2e: the same metric through the request server (gpsm_server_*), host
+buffers in and every embedding row copied back to host memory, all inside
+the timed region.
 
 --impl reference times the CPU port of the reference pipeline (the oracle's
 restated filter, refinement, candidate edges and plain-order joins) on all
@@ -189,9 +192,18 @@ def run_ours(args):
     packed = G.pack_queries(wl.queries)
     nq = len(wl.queries)
     cap = args.cap
+    model = None
+    if args.order == "learned":
+        from gpsm_b200 import learned as L
+        model = L.load(local)
+    orders = "learned" if args.order == "learned" else None
+
+    def run_step(slots):
+        return G.match_batch(dg, wl.queries, cap=cap, packed=packed, slots=slots, orders=orders, model=model)
+
     # warm-up
     for _ in range(args.warmup):
-        G.match_batch(dg, wl.queries, cap=cap, packed=packed)
+        run_step(args.slots)
     clocks = ClockSampler(local)
     step_ms, qms_all, launches, rows_total = [], [], 0, 0
     alg_bytes, expand_ms, expand_launches = 0, 0.0, 0
@@ -200,7 +212,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         G.flush_l2(256 << 20)
-        counts, capped, qms, info = G.match_batch(dg, wl.queries, cap=cap, packed=packed)
+        counts, capped, qms, info = run_step(args.slots)
         step_ms.append(info["device_ms"])
         qms_all.extend(qms.tolist())
         launches += info["launches"]
@@ -214,17 +226,28 @@ def run_ours(args):
     dev_s = max_over_ranks(pg, sum(step_ms) / 1e3)
     total_q = sum_over_ranks(pg, nq * args.steps)
     total_rows = sum_over_ranks(pg, rows_total)
-    # e2e: the public C ABI per query, host buffers, rows copied back
+    # the plain GpSM-order path (one slot), one step, for the ratio
+    plain_ms = None
+    if not args.no_plain:
+        G.flush_l2(256 << 20)
+        pc, _, _, pinfo = G.match_batch(dg, wl.queries, cap=cap, packed=packed, slots=1)
+        plain_ms = max_over_ranks(pg, pinfo["device_ms"])
+        plain_rows = pinfo["rows"]
+    # e2e: the request server with host buffers; rows come back to the host
     h2d = sum(int(q.labels.nbytes + q.edges.nbytes) for q in wl.queries)
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = 1
     barrier(pg)
+    srv = G.Server(dg, slots=args.slots, cap=cap, order=args.order if args.order == "learned" else None,
+                   model=model, collect_rows=True)
     t1 = time.perf_counter()
     d2h = 0
     for _ in range(e2e_steps):
-        for q in wl.queries:
-            out = G.match(dg, q, cap=cap)
-            d2h += out.rows.nbytes
+        tickets = [srv.submit(q) for q in wl.queries]
+        for t in tickets:
+            r = srv.wait(t)
+            d2h += r["embeddings"].nbytes
     e2e_wall = max_over_ranks(pg, time.perf_counter() - t1)
+    srv.close()
     d2h //= e2e_steps
     e2e_q = sum_over_ranks(pg, nq * e2e_steps)
     peak, peak_kind = peaks()
@@ -251,13 +274,17 @@ def run_ours(args):
             "data": "synthetic",
             "config": {"workload": args.workload + ": " + WORKLOADS.get(args.workload, ""),
                        "queries_per_step_per_gpu": nq, "embedding_cap": cap, "order": args.order,
-                       "l2": "flushed (256 MiB write) between steps", "parallelism": f"replicas x{world}"},
+                       "slots": args.slots, "l2": "flushed (256 MiB write) between steps",
+                       "parallelism": f"replicas x{world}"},
+            "plain_order": None if plain_ms is None else {
+                "value": total_q / args.steps / (plain_ms / 1e3), "unit": "queries/s", "ms_per_step": plain_ms,
+                "slots": 1, "embeddings_per_s": plain_rows / (plain_ms / 1e3)},
             "embeddings_per_s": total_rows / dev_s,
             "p50_ms": float(np.percentile(qms_all, 50)) if qms_all else None,
             "p99_ms": float(np.percentile(qms_all, 99)) if qms_all else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "kernel": "k_expand", "peak_source": peak_kind,
+                         "kernel": "join step (k_locate + k_extend)", "peak_source": peak_kind,
                          "expand_launches": expand_launches, "expand_ms": expand_ms},
             "cpu_baseline": None if cpu_rate is None else {
                 "value": cpu_rate, "unit": "queries/s", "cores": cores, "kind": "port",
@@ -323,7 +350,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat20")
-    ap.add_argument("--order", default="plain", choices=["plain"])
+    ap.add_argument("--order", default="learned", choices=["plain", "learned"])
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-order comparison step")
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--first", type=int, default=0, help="first query of the batch (profiling subsets)")

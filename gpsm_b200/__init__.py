@@ -20,13 +20,41 @@ from . import _lib
 from ._lib import GpsmError  # noqa: F401
 
 __all__ = ["init", "shutdown", "DeviceGraph", "Engine", "match", "match_batch", "flush_l2", "MatchOutput",
-           "debug_filter", "GpsmError", "pack_queries"]
+           "debug_filter", "GpsmError", "pack_queries", "Model", "order_features", "last_levels", "Server",
+           "set_tuning", "get_tuning"]
 
 
-def init(device=0, arena_bytes=0):
-    """Select the device and create the default engine (Match::initGPU)."""
+import json as _json
+import os as _os
+
+TUNING_FILE = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "data", "tuning.json")
+
+
+def init(device=0, arena_bytes=0, tuning_file=TUNING_FILE):
+    """Select the device and create the default engine (Match::initGPU).
+    Applies the autotuner's choices when tuning_file exists."""
     lib = _lib.load()
+    if tuning_file and _os.path.exists(tuning_file):
+        set_tuning(**_json.load(open(tuning_file)).get("choice", {}))
     _lib.check(lib.gpsm_init_ex(device, arena_bytes), "gpsm_init")
+
+
+def set_tuning(**kw):
+    """Process-wide launch choices: heavy_degree, ext_blocks_per_sm,
+    step_cands, level_bytes, slots (unset or 0 = unchanged)."""
+    lib = _lib.load()
+    t = _lib.Tuning()
+    for k, v in kw.items():
+        if k in dict(_lib.Tuning._fields_):
+            setattr(t, k, int(v))
+    _lib.check(lib.gpsm_set_tuning(C.byref(t)), "gpsm_set_tuning")
+
+
+def get_tuning():
+    lib = _lib.load()
+    t = _lib.Tuning()
+    _lib.check(lib.gpsm_get_tuning(C.byref(t)), "gpsm_get_tuning")
+    return {k: getattr(t, k) for k, _ in _lib.Tuning._fields_ if k != "pad"}
 
 
 def shutdown():
@@ -110,19 +138,28 @@ def _query_arrays(query):
 
 
 def match(dgraph, query, cap=None, order=None, count_only=False, keep_on_device=False, engine=None,
-          level_bytes=0, result_rows=0):
+          level_bytes=0, result_rows=0, model=None, memory_budget=0, work_cap=0):
     """Match one query (Match::match). order: None = the reference's plain
-    join order, else pos2id (a connected vertex order)."""
+    join order, a pos2id list (a connected vertex order), or "learned" (the
+    order chosen by `model`, falling back to the plain order when its
+    predicted peak table exceeds memory_budget bytes)."""
     lib = _lib.load()
     qn = query.n
     ql, qe = _query_arrays(query)
     opts = _lib.MatchOpts()
     opts.cap = int(cap or 0)
     order_arr = None
-    if order is not None:
+    if isinstance(order, str) and order == "learned":
+        if model is None:
+            raise ValueError("order='learned' needs a model")
+        opts.order_mode = _lib.GPSM_ORDER_LEARNED
+        opts.model = model.handle
+    elif order is not None:
         order_arr = np.ascontiguousarray(order, dtype=np.int32)
         opts.order_mode = _lib.GPSM_ORDER_GIVEN
         opts.order = order_arr.ctypes.data
+    opts.memory_budget = int(memory_budget)
+    opts.work_cap = int(work_cap)
     opts.level_bytes = int(level_bytes)
     opts.result_rows = int(result_rows)
     opts.flags = (_lib.GPSM_F_COUNT_ONLY if count_only else 0) | (_lib.GPSM_F_KEEP_ON_DEVICE if keep_on_device else 0)
@@ -181,8 +218,11 @@ def pack_queries(queries):
     return voff, ql, eoff, qe
 
 
-def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None, level_bytes=0):
-    """Match queries back to back on one engine (rows stay on the device).
+def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None, level_bytes=0, slots=1,
+                model=None, slot_arena=0):
+    """Match queries back to back (rows stay on the device); slots > 1 runs
+    them on that many engine slots at once (continuous batching); orders:
+    None (plain), "learned" (model) or a list of pos2id per query.
     Returns (counts, capped, per-query device ms, batch info dict)."""
     lib = _lib.load()
     voff, ql, eoff, qe = packed if packed is not None else pack_queries(queries)
@@ -191,7 +231,10 @@ def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None
     opts.cap = int(cap or 0)
     opts.level_bytes = int(level_bytes)
     ords = None
-    if orders is not None:
+    if isinstance(orders, str) and orders == "learned":
+        opts.order_mode = _lib.GPSM_ORDER_LEARNED
+        opts.model = model.handle
+    elif orders is not None:
         ords = np.ascontiguousarray(np.concatenate([np.asarray(o, np.int32) for o in orders]), np.int32)
         opts.order_mode = _lib.GPSM_ORDER_GIVEN
     counts = np.zeros(nq, np.uint64)
@@ -199,9 +242,14 @@ def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None
     qms = np.zeros(nq, np.float64)
     info = _lib.BatchInfo()
     eng = engine.handle if engine is not None else None
-    rc = lib.gpsm_match_batch(eng, dgraph.handle, nq, _lib.ptr(voff), _lib.ptr(ql), _lib.ptr(eoff), _lib.ptr(qe),
-                              C.byref(opts), _lib.ptr(ords), _lib.ptr(counts), _lib.ptr(capped), _lib.ptr(qms),
-                              C.byref(info))
+    if slots > 1:
+        rc = lib.gpsm_match_batch_parallel(dgraph.handle, nq, _lib.ptr(voff), _lib.ptr(ql), _lib.ptr(eoff),
+                                           _lib.ptr(qe), C.byref(opts), _lib.ptr(ords), slots, int(slot_arena),
+                                           _lib.ptr(counts), _lib.ptr(capped), _lib.ptr(qms), C.byref(info))
+    else:
+        rc = lib.gpsm_match_batch(eng, dgraph.handle, nq, _lib.ptr(voff), _lib.ptr(ql), _lib.ptr(eoff), _lib.ptr(qe),
+                                  C.byref(opts), _lib.ptr(ords), _lib.ptr(counts), _lib.ptr(capped), _lib.ptr(qms),
+                                  C.byref(info))
     _lib.check(rc, "gpsm_match_batch")
     d = {k: getattr(info, k) for k, _ in _lib.BatchInfo._fields_}
     return counts, capped.astype(bool), qms, d
@@ -211,3 +259,160 @@ def flush_l2(nbytes=256 << 20, engine=None):
     lib = _lib.load()
     eng = engine.handle if engine is not None else None
     _lib.check(lib.gpsm_flush_l2(eng, int(nbytes)), "gpsm_flush_l2")
+
+
+class Model:
+    """The learned join-order MLP (16 -> 64 -> 64 -> 1, BF16 weights, FP32
+    accumulation) on one device; training and inference run on the GPU."""
+
+    def __init__(self, device=0, seed=0, params=None):
+        lib = _lib.load()
+        self._lib = lib
+        self.n_params = lib.gpsm_model_params()
+        h = _lib.vp()
+        _lib.check(lib.gpsm_model_create(device, seed, C.byref(h)), "gpsm_model_create")
+        self.handle = h
+        if params is not None:
+            self.set(params)
+
+    def set(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == self.n_params
+        _lib.check(self._lib.gpsm_model_set(self.handle, _lib.ptr(p)), "gpsm_model_set")
+
+    def get(self):
+        p = np.zeros(self.n_params, np.float32)
+        _lib.check(self._lib.gpsm_model_get(self.handle, _lib.ptr(p)), "gpsm_model_get")
+        return p
+
+    def train(self, x, y, epochs=30, batch=2048, lr=2e-3, seed=0):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = C.c_float(0)
+        _lib.check(self._lib.gpsm_model_train(self.handle, _lib.ptr(x), _lib.ptr(y), len(y), epochs, batch, lr, seed,
+                                              C.byref(loss)), "gpsm_model_train")
+        return loss.value
+
+    def grad(self, x, y):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float(0)
+        _lib.check(self._lib.gpsm_model_grad(self.handle, _lib.ptr(x), _lib.ptr(y), len(y), _lib.ptr(g),
+                                             C.byref(loss)), "gpsm_model_grad")
+        return loss.value, g
+
+    def predict(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros(len(x), np.float32)
+        _lib.check(self._lib.gpsm_model_predict(self.handle, _lib.ptr(x), len(x), _lib.ptr(y)), "gpsm_model_predict")
+        return y
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self._lib.gpsm_model_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def order_features(dgraph, query, filt, pos2id):
+    """Features of every join step of the order pos2id ((n-1, 16) float32),
+    from debug_filter()'s statistics."""
+    lib = _lib.load()
+    ql, qe = _query_arrays(query)
+    out = np.zeros((max(query.n - 1, 1), 16), np.float32)
+    cc = np.ascontiguousarray(filt["cand_count"], np.uint32)
+    sf = np.ascontiguousarray(filt["size_fwd"], np.uint64)
+    sr = np.ascontiguousarray(filt["size_rev"], np.uint64)
+    if sf.size == 0:
+        sf = np.zeros(1, np.uint64)
+        sr = np.zeros(1, np.uint64)
+    po = np.ascontiguousarray(pos2id, np.int32)
+    _lib.check(lib.gpsm_order_features(dgraph.handle, query.n, _lib.ptr(ql), query.m, _lib.ptr(qe), _lib.ptr(cc),
+                                       _lib.ptr(sf), _lib.ptr(sr), _lib.ptr(po), _lib.ptr(out)), "gpsm_order_features")
+    return out[: query.n - 1]
+
+
+def last_levels(n, engine=None):
+    """(rows extended, candidates scanned, rows produced) per table width 0..n
+    of the engine's last match."""
+    lib = _lib.load()
+    a = np.zeros(n + 1, np.uint64)
+    b = np.zeros(n + 1, np.uint64)
+    c = np.zeros(n + 1, np.uint64)
+    eng = engine.handle if engine is not None else None
+    _lib.check(lib.gpsm_last_levels(eng, n, _lib.ptr(a), _lib.ptr(b), _lib.ptr(c)), "gpsm_last_levels")
+    return a, b, c
+
+
+class Server:
+    """Request loop over `slots` engine slots: submit() returns at once,
+    wait() blocks until the request is done. Requests are admitted to their
+    joins when their predicted join memory fits memory_budget bytes."""
+
+    def __init__(self, dgraph, slots=4, memory_budget=0, slot_arena=0, cap=None, order=None, model=None,
+                 collect_rows=False):
+        lib = _lib.load()
+        self._lib = lib
+        opts = _lib.MatchOpts()
+        opts.cap = int(cap or 0)
+        if order == "learned":
+            opts.order_mode = _lib.GPSM_ORDER_LEARNED
+            opts.model = model.handle
+        self._model = model  # keep alive
+        h = _lib.vp()
+        _lib.check(lib.gpsm_server_create(dgraph.handle, slots, int(memory_budget), int(slot_arena), C.byref(opts),
+                                          1 if collect_rows else 0, C.byref(h)), "gpsm_server_create")
+        self.handle = h
+        self.collect = collect_rows
+
+    def submit(self, query):
+        ql, qe = _query_arrays(query)
+        t = C.c_uint64(0)
+        _lib.check(self._lib.gpsm_server_submit(self.handle, query.n, _lib.ptr(ql), query.m, _lib.ptr(qe),
+                                                C.byref(t)), "gpsm_server_submit")
+        return t.value, query.n
+
+    def wait(self, ticket, timeout=-1.0):
+        tid, qn = ticket
+        info = _lib.RequestInfo()
+        out = _lib.vp()
+        idm = np.zeros(qn, np.int32)
+        rc = self._lib.gpsm_server_wait(self.handle, tid, float(timeout), C.byref(info),
+                                        C.byref(out) if self.collect else None, _lib.ptr(idm))
+        _lib.check(rc, "gpsm_server_wait")
+        d = {k: getattr(info, k) for k, _ in _lib.RequestInfo._fields_}
+        rows = None
+        if self.collect:
+            n = int(info.rows)
+            if out.value and n:
+                buf = (C.c_uint32 * (n * qn)).from_address(out.value)
+                rows = np.frombuffer(buf, dtype=np.uint32).copy().reshape(n, qn)
+                self._lib.gpsm_free(out)
+            else:
+                rows = np.zeros((0, qn), np.uint32)
+            d["id_map"] = idm
+            d["embeddings"] = rows[:, idm] if len(rows) else rows
+        return d
+
+    def stats(self):
+        v = [C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint32(), C.c_uint32()]
+        _lib.check(self._lib.gpsm_server_stats(self.handle, *[C.byref(x) for x in v]), "gpsm_server_stats")
+        return dict(in_use=v[0].value, peak_in_use=v[1].value, budget=v[2].value, queued=v[3].value,
+                    active=v[4].value)
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self._lib.gpsm_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

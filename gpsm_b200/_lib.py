@@ -44,6 +44,12 @@ SIGNATURES = {
     "gpsm_csr_from_edges": (C.c_int, [u32, u64, vp, vp, vp]),
     "gpsm_gen_query": (i64, [u32, vp, vp, vp, u32, C.c_int, f64, f64, u64, vp, vp, vp]),
     "gpsm_last_error": (C.c_char_p, []),
+    "gpsm_text_open": (C.c_int, [C.c_char_p, vp]),
+    "gpsm_text_count": (C.c_int, [vp, vp]),
+    "gpsm_text_graph_info": (C.c_int, [vp, u32, vp, vp, vp]),
+    "gpsm_text_graph_read": (C.c_int, [vp, u32, vp, vp, vp]),
+    "gpsm_text_close": (C.c_int, [vp]),
+    "gpsm_text_write": (C.c_int, [C.c_char_p, C.c_int, i32, u32, vp, u64, vp, vp, C.c_int]),
     "gpsm_init": (C.c_int, [C.c_int]),
     "gpsm_init_ex": (C.c_int, [C.c_int, u64]),
     "gpsm_shutdown": (C.c_int, []),
@@ -62,6 +68,14 @@ SIGNATURES = {
     "gpsm_select_vertices": (C.c_int, [vp, vp, vp, u32, u32, u32, vp, vp]),
     "gpsm_select_vertices_static": (C.c_int, [vp, vp, u32, u32, u32, vp, vp, vp]),
     "gpsm_last_levels": (C.c_int, [vp, u32, vp, vp, vp]),
+    "gpsm_match_batch_parallel": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u64, vp, vp, vp, vp]),
+    "gpsm_server_create": (C.c_int, [vp, u32, u64, u64, vp, i32, vp]),
+    "gpsm_server_submit": (C.c_int, [vp, u32, vp, u32, vp, vp]),
+    "gpsm_server_wait": (C.c_int, [vp, u64, f64, vp, vp, vp]),
+    "gpsm_server_stats": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "gpsm_server_destroy": (C.c_int, [vp]),
+    "gpsm_set_tuning": (C.c_int, [vp]),
+    "gpsm_get_tuning": (C.c_int, [vp]),
     "gpsm_model_params": (C.c_int, []),
     "gpsm_model_create": (C.c_int, [C.c_int, u64, vp]),
     "gpsm_model_destroy": (C.c_int, [vp]),
@@ -89,6 +103,16 @@ class MatchInfo(C.Structure):
                 ("expand_launches", u64), ("filter_launches", u64), ("alg_bytes_join", u64),
                 ("expand_ms", f64), ("plan_ms", f64), ("predicted_work", f64), ("predicted_peak", f64),
                 ("order_fallback", i32), ("aborted", i32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("heavy_degree", u32), ("ext_blocks_per_sm", u32), ("step_cands", u64), ("level_bytes", u64),
+                ("slots", u32), ("pad", u32)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", i32), ("capped", i32), ("rows", u64), ("submit_ms", f64), ("start_ms", f64),
+                ("admit_ms", f64), ("end_ms", f64), ("device_ms", f64), ("admitted_bytes", u64)]
 
 
 class BatchInfo(C.Structure):

@@ -1,0 +1,74 @@
+"""Autotuner for the engine's launch choices.
+
+    python -m gpsm_b200.autotune [--workload rmat20] [--queries 24] [--out gpsm_b200/data/tuning.json]
+
+Times a sample of the workload's queries (device time of the whole batch,
+best of two runs after a warm-up) under every combination of:
+  heavy_degree       candidates above it get a block each (filter kernels)
+  ext_blocks_per_sm  persistent join-extend blocks per SM
+  step_cands         candidates one join step may admit
+  slots              engine slots running queries at once
+and writes the fastest combination to --out; gpsm_b200.init() applies it.
+Queries whose plain-order joins blow up are left out of the sample (they
+measure the order, not the launch shapes): the sample keeps queries whose
+device time under the default choices is below --max-ms.
+"""
+import argparse
+import itertools
+import json
+import os
+import time
+
+import numpy as np
+
+from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
+from . import workloads as W
+
+GRID = dict(heavy_degree=[256, 1024, 4096], ext_blocks_per_sm=[4, 8], step_cands=[1 << 23, 1 << 25],
+            slots=[1, 2, 4, 8])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="rmat20")
+    ap.add_argument("--queries", type=int, default=24)
+    ap.add_argument("--cap", type=int, default=10_000_000)
+    ap.add_argument("--max-ms", type=float, default=200.0)
+    ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                                                  "tuning.json"))
+    args = ap.parse_args()
+    init(0, tuning_file=None)
+    default = get_tuning()
+    wl = W.workload(args.workload, count=max(args.queries * 3, 100))
+    dg = DeviceGraph(wl.graph)
+    sample = []
+    for q in wl.queries:
+        out = match(dg, q, cap=args.cap, count_only=True)
+        if out.info["device_ms"] < args.max_ms:
+            sample.append(q)
+        if len(sample) >= args.queries:
+            break
+    results = []
+    keys = list(GRID)
+    for combo in itertools.product(*[GRID[k] for k in keys]):
+        choice = dict(zip(keys, combo))
+        set_tuning(**choice)
+        match_batch(dg, sample, cap=args.cap, slots=choice["slots"])  # warm-up
+        best = min(match_batch(dg, sample, cap=args.cap, slots=choice["slots"])[3]["device_ms"] for _ in range(2))
+        results.append(dict(choice=choice, device_ms=best))
+        print(json.dumps(results[-1]), flush=True)
+    set_tuning(**default)
+    best = min(results, key=lambda r: r["device_ms"])
+    base = [r for r in results if all(r["choice"][k] == default.get(k, r["choice"][k]) for k in keys)]
+    out = dict(choice=best["choice"], device_ms=best["device_ms"],
+               default_ms=base[0]["device_ms"] if base else None, workload=args.workload,
+               sample_queries=len(sample), cap=args.cap, when=time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
+               all=results)
+    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    with open(args.out, "w") as f:
+        json.dump(out, f, indent=1)
+    print("best", json.dumps(best), "default", out["default_ms"], flush=True)
+
+
+if __name__ == "__main__":
+    main()

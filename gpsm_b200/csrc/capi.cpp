@@ -16,22 +16,7 @@
 
 using namespace gpsm;
 
-struct gpsm_graph_s {
-  DeviceGraph* g;
-};
-
-struct gpsm_model_s {
-  Model* m;
-};
-
-struct gpsm_engine_s {
-  Workspace* ws = nullptr;
-  std::mutex mu;
-  // state kept by the last filter-only call, for the debug entry points
-  QueryPlan last_plan;
-  MatchResult last;
-  std::vector<uint32_t*> last_lists;
-};
+#include "handles.h"
 
 namespace {
 
@@ -71,7 +56,9 @@ uint64_t default_arena_bytes() {
 
 gpsm_engine_s* engine_or_default(gpsm_engine_t e) { return e ? e : g_default; }
 
-MatchOptions to_options(const gpsm_match_opts* o) {
+}  // namespace
+
+MatchOptions gpsm::options_from(const gpsm_match_opts* o) {
   MatchOptions m;
   if (!o) return m;
   m.cap = o->cap ? o->cap : ~0ULL;
@@ -90,6 +77,16 @@ MatchOptions to_options(const gpsm_match_opts* o) {
   m.work_cap = o->work_cap;
   return m;
 }
+
+int gpsm::error_from(const CudaError& e) {
+  if (e.err == cudaErrorMemoryAllocation) return GPSM_ERR_NOMEM;
+  if (e.err == cudaErrorInvalidValue) return GPSM_ERR_INVALID;
+  return GPSM_ERR_CUDA;
+}
+
+namespace {
+
+MatchOptions to_options(const gpsm_match_opts* o) { return options_from(o); }
 
 void fill_info(const MatchResult& R, gpsm_match_info* info) {
   if (!info) return;
@@ -307,6 +304,28 @@ int gpsm_last_levels(gpsm_engine_t eng, uint32_t n, uint64_t* level_in, uint64_t
     if (level_cands) level_cands[w] = w < st.level_cands.size() ? st.level_cands[w] : 0;
     if (level_out) level_out[w] = w < st.level_rows.size() ? st.level_rows[w] : 0;
   }
+  return GPSM_OK;
+}
+
+int gpsm_set_tuning(const gpsm_tuning* t) {
+  if (!t) return GPSM_ERR_INVALID;
+  Tuning& T = tuning();
+  if (t->heavy_degree) T.heavy_degree = t->heavy_degree;
+  if (t->ext_blocks_per_sm) T.ext_blocks_per_sm = std::min<uint32_t>(t->ext_blocks_per_sm, 8);
+  if (t->step_cands) T.step_cands = std::max<uint64_t>(t->step_cands, 1u << 16);
+  if (t->level_bytes) T.level_bytes = std::max<uint64_t>(t->level_bytes, 1u << 20);
+  if (t->slots) T.slots = std::min<uint32_t>(t->slots, 64);
+  return GPSM_OK;
+}
+
+int gpsm_get_tuning(gpsm_tuning* t) {
+  if (!t) return GPSM_ERR_INVALID;
+  const Tuning& T = tuning();
+  t->heavy_degree = T.heavy_degree;
+  t->ext_blocks_per_sm = T.ext_blocks_per_sm;
+  t->step_cands = T.step_cands;
+  t->level_bytes = T.level_bytes;
+  t->slots = T.slots;
   return GPSM_OK;
 }
 

@@ -576,6 +576,36 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     GPSM_CUDA(cudaStreamSynchronize(s));
     return GPSM_OK;
   }
+  // join memory: level buffers, step scratch and the result buffer are the
+  // most the joins can hold; a learned plan predicts how much of it is used
+  struct AdmitGuard {
+    const MatchOptions& o;
+    uint64_t bytes = 0;
+    ~AdmitGuard() {
+      if (bytes && o.release) o.release(o.admit_ctx, bytes);
+    }
+  } admit_guard{opt};
+  if (opt.admit) {
+    const uint64_t min_rows_a = (uint64_t)g.max_degree + 64;
+    uint64_t cap_bytes = 0;
+    for (uint32_t w = 2; w < qn; ++w)
+      cap_bytes += std::max<uint64_t>(opt.level_bytes, min_rows_a * 4ull * w);
+    const uint64_t res_rows =
+        std::max<uint64_t>(std::min<uint64_t>(std::max<uint64_t>(opt.result_rows, opt.keep_on_device ? opt.cap : 0),
+                                              opt.cap),
+                           1);
+    const uint64_t res_bytes = res_rows * 4ull * qn;
+    cap_bytes += res_bytes + (1ull << 30);
+    uint64_t want = cap_bytes;
+    if (opt.order_mode == ORDER_LEARNED && !R.stats.order_fallback && R.stats.predicted_peak > 0)
+      want = std::min<uint64_t>(cap_bytes, (uint64_t)R.stats.predicted_peak + res_bytes + (64ull << 20));
+    if (!opt.admit(opt.admit_ctx, want)) {
+      set_last_error("admission refused: predicted join memory does not fit the budget");
+      return GPSM_ERR_BUDGET;
+    }
+    admit_guard.bytes = want;
+    R.stats.admitted_bytes = want;
+  }
 
   // ---- joins ---------------------------------------------------------------------
   // back-neighbour descriptors for each added position p >= 1

@@ -54,16 +54,22 @@ struct MatchOptions {
   uint64_t cap = ~0ULL;            // embedding cap (rows after which the query stops)
   int order_mode = ORDER_PLAIN;
   std::vector<int32_t> given_order;  // pos2id when ORDER_GIVEN
-  uint64_t level_bytes = 256ull << 20;  // per intermediate level buffer
+  uint64_t level_bytes = tuning().level_bytes;  // per intermediate level buffer
   uint64_t result_rows = 1ull << 22;    // device result buffer rows before flushing to host
   uint64_t step_rows = 1ull << 22;      // input rows one join step may look at
-  uint64_t step_cands = 1ull << 25;     // candidates one join step may admit
+  uint64_t step_cands = tuning().step_cands;  // candidates one join step may admit
   bool keep_on_device = false;          // never flush: fail with GPSM_ERR_BUDGET instead
   bool collect_rows = true;             // false: count only (result rows are discarded)
   bool filter_only = false;             // stop after the join order (debug entry points)
   Model* model = nullptr;               // ORDER_LEARNED
   uint64_t memory_budget = 0;           // bytes; predicted peak above it -> plain order (0 = arena size)
   uint64_t work_cap = 0;                // candidates the joins may scan before stopping (0 = none)
+  // Admission hook (serving): called after the order is chosen, before the
+  // joins, with the bytes the joins are predicted to use; returns false to
+  // refuse (GPSM_ERR_BUDGET). release() gets the same bytes back afterwards.
+  bool (*admit)(void* ctx, uint64_t bytes) = nullptr;
+  void (*release)(void* ctx, uint64_t bytes) = nullptr;
+  void* admit_ctx = nullptr;
 };
 
 struct MatchStats {
@@ -81,6 +87,7 @@ struct MatchStats {
   double plan_ms = 0;           // learned-order planning (host wall time incl. the planner kernel)
   double predicted_work = 0, predicted_peak = 0;
   bool order_fallback = false;  // learned order rejected by the memory budget
+  uint64_t admitted_bytes = 0;  // bytes granted by the admission hook
   bool aborted = false;         // work cap reached
   uint64_t alg_bytes_filter = 0;
 };

@@ -92,11 +92,26 @@ __global__ void __launch_bounds__(kCompactBlock) k_compact(const uint32_t* __res
 // Warp per candidate mu of u. For each target v (label, degree) in order:
 // every neighbour mv of mu with that label and degree >= deg(v) enters C(v);
 // if none does, mu leaves C(u) and later targets are skipped.
+// Candidates with more than kHeavyDegree neighbours are handed to a block
+// per candidate (the *_heavy kernels) through a per-launch list, so one hub
+// does not hold a warp for thousands of iterations while the grid idles.
+constexpr uint32_t kHeavyBlock = 512;
+
+__device__ __forceinline__ bool defer_heavy(uint32_t deg, uint32_t item, HeavyList hl) {
+  if (deg <= hl.threshold || hl.items == nullptr) return false;
+  uint32_t slot = 0;
+  if ((threadIdx.x & 31) == 0) slot = atomicAdd(hl.count, 1u);
+  slot = __shfl_sync(0xffffffffu, slot, 0);
+  if (slot >= hl.cap) return false;  // list full: the warp does it
+  if ((threadIdx.x & 31) == 0) hl.items[slot] = item;
+  return true;
+}
+
 __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __restrict__ list,
                                                  const uint32_t* __restrict__ count, uint32_t u,
                                                  const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                  uint32_t* __restrict__ bm, uint32_t words,
-                                                 const uint32_t* __restrict__ flags) {
+                                                 const uint32_t* __restrict__ flags, HeavyList hl) {
   extern __shared__ uint32_t s_tgt[];  // 3 * ntgt: v, label, degree
   for (uint32_t i = threadIdx.x; i < 3 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
@@ -108,6 +123,7 @@ __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __
   for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
     const uint32_t mu = list[w];
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    if (defer_heavy(e - b, mu, hl)) continue;
     for (uint32_t t = 0; t < ntgt; ++t) {
       const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
       uint32_t* bmv = bm + (size_t)v * words;
@@ -128,13 +144,45 @@ __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __
   }
 }
 
+// Block per deferred candidate: the same steps as k_explore with a
+// block-wide vote per target.
+__global__ void __launch_bounds__(kHeavyBlock) k_explore_heavy(GraphView g, HeavyList hl, uint32_t u,
+                                                               const uint32_t* __restrict__ tgt, uint32_t ntgt,
+                                                               uint32_t* __restrict__ bm, uint32_t words,
+                                                               const uint32_t* __restrict__ flags) {
+  if (*flags & DF_EMPTY) return;
+  const uint32_t n = min(*hl.count, hl.cap);
+  uint32_t* bmu = bm + (size_t)u * words;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t mu = hl.items[i];
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    for (uint32_t t = 0; t < ntgt; ++t) {
+      const uint32_t v = tgt[3 * t], lv = tgt[3 * t + 1], dv = tgt[3 * t + 2];
+      uint32_t* bmv = bm + (size_t)v * words;
+      bool any = false;
+      for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+        const uint32_t mv = g.col[j];
+        const uint2 ld = g.labdeg[mv];
+        if (ld.x == lv && ld.y >= dv) {
+          atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
+          any = true;
+        }
+      }
+      if (!__syncthreads_or(any)) {
+        if (threadIdx.x == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        break;
+      }
+    }
+  }
+}
+
 // Warp per candidate mu of u: mu stays only if every target v has a
 // candidate among mu's neighbours.
 __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __restrict__ list,
                                                 const uint32_t* __restrict__ count, uint32_t u,
                                                 const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                 uint32_t* __restrict__ bm, uint32_t words,
-                                                const uint32_t* __restrict__ flags) {
+                                                const uint32_t* __restrict__ flags, HeavyList hl) {
   extern __shared__ uint32_t s_tgt[];
   for (uint32_t i = threadIdx.x; i < ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
@@ -146,6 +194,7 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
   for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
     const uint32_t mu = list[w];
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    if (defer_heavy(e - b, mu, hl)) continue;
     for (uint32_t t = 0; t < ntgt; ++t) {
       const uint32_t* bmv = bm + (size_t)s_tgt[t] * words;
       bool found = false;
@@ -169,6 +218,36 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
   }
 }
 
+__global__ void __launch_bounds__(kHeavyBlock) k_refine_heavy(GraphView g, HeavyList hl, uint32_t u,
+                                                              const uint32_t* __restrict__ tgt, uint32_t ntgt,
+                                                              uint32_t* __restrict__ bm, uint32_t words,
+                                                              const uint32_t* __restrict__ flags) {
+  if (*flags & DF_EMPTY) return;
+  const uint32_t n = min(*hl.count, hl.cap);
+  uint32_t* bmu = bm + (size_t)u * words;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t mu = hl.items[i];
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    for (uint32_t t = 0; t < ntgt; ++t) {
+      const uint32_t* bmv = bm + (size_t)tgt[t] * words;
+      bool found = false;
+      for (uint32_t j0 = b; j0 < e && !found; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        bool hit = false;
+        if (j < e) {
+          const uint32_t mv = g.col[j];
+          hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+        }
+        found = __syncthreads_or(hit);
+      }
+      if (!found) {
+        if (threadIdx.x == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        break;
+      }
+    }
+  }
+}
+
 // Work item i belongs to edge-direction d with item_base[d] <= i < item_base[d+1].
 __device__ __forceinline__ uint32_t find_dir(const unsigned long long* __restrict__ s_base, uint32_t ndir,
                                              unsigned long long i) {
@@ -185,7 +264,7 @@ __device__ __forceinline__ uint32_t find_dir(const unsigned long long* __restric
 __global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir* __restrict__ dirs,
                                                      uint32_t ndir, const unsigned long long* __restrict__ s_base,
                                                      const uint32_t* __restrict__ bm, uint32_t words,
-                                                     uint32_t* __restrict__ cnt) {
+                                                     uint32_t* __restrict__ cnt, HeavyList hl) {
   const unsigned long long items = s_base[ndir];
   const uint32_t lane = threadIdx.x & 31;
   const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
@@ -195,6 +274,7 @@ __global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
     uint32_t c = 0;
     for (uint32_t j = b + lane; j < e; j += 32) {
       const uint32_t mv = g.col[j];
@@ -210,7 +290,7 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
                                                      uint32_t ndir, const unsigned long long* __restrict__ s_base,
                                                      const uint32_t* __restrict__ bm, uint32_t words,
                                                      const unsigned long long* __restrict__ goff,
-                                                     uint32_t* __restrict__ nbrs) {
+                                                     uint32_t* __restrict__ nbrs, HeavyList hl) {
   const unsigned long long items = s_base[ndir];
   const uint32_t lane = threadIdx.x & 31;
   const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
@@ -220,6 +300,7 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
     unsigned long long pos = goff[w];
     for (uint32_t j0 = b; j0 < e; j0 += 32) {
       const uint32_t j = j0 + lane;
@@ -232,6 +313,87 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
       const uint32_t bal = __ballot_sync(0xffffffffu, hit);
       if (hit) nbrs[pos + __popc(bal & ((1u << lane) - 1))] = mv;
       pos += __popc(bal);
+    }
+  }
+}
+
+// Block per deferred (direction, candidate) item: the count as a block sum.
+__global__ void __launch_bounds__(kHeavyBlock) k_cedge_count_heavy(GraphView g, const CedgeDir* __restrict__ dirs,
+                                                                   uint32_t ndir,
+                                                                   const unsigned long long* __restrict__ s_base,
+                                                                   const uint32_t* __restrict__ bm, uint32_t words,
+                                                                   uint32_t* __restrict__ cnt, HeavyList hl) {
+  __shared__ uint32_t s_part[kHeavyBlock / 32];
+  const uint32_t n = min(*hl.count, hl.cap);
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t w = hl.items[i];
+    const uint32_t d = find_dir(s_base, ndir, w);
+    const CedgeDir cd = dirs[d];
+    const uint32_t mu = cd.ids[w - cd.item_base];
+    const uint32_t* bmv = bm + (size_t)cd.v * words;
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    uint32_t c = 0;
+    for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+      const uint32_t mv = g.col[j];
+      c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (uint32_t k = 0; k < blockDim.x / 32; ++k) t += s_part[k];
+      cnt[w] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Block per deferred item: N(mu) ∩ C(v) written in adjacency order; each
+// chunk of blockDim neighbours is compacted with warp ballots and a scan of
+// the warp totals.
+__global__ void __launch_bounds__(kHeavyBlock) k_cedge_write_heavy(GraphView g, const CedgeDir* __restrict__ dirs,
+                                                                   uint32_t ndir,
+                                                                   const unsigned long long* __restrict__ s_base,
+                                                                   const uint32_t* __restrict__ bm, uint32_t words,
+                                                                   const unsigned long long* __restrict__ goff,
+                                                                   uint32_t* __restrict__ nbrs, HeavyList hl) {
+  __shared__ uint32_t s_warp[kHeavyBlock / 32];
+  __shared__ uint32_t s_total;
+  const uint32_t n = min(*hl.count, hl.cap);
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x / 32;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t w = hl.items[i];
+    const uint32_t d = find_dir(s_base, ndir, w);
+    const CedgeDir cd = dirs[d];
+    const uint32_t mu = cd.ids[w - cd.item_base];
+    const uint32_t* bmv = bm + (size_t)cd.v * words;
+    const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    unsigned long long pos = goff[w];
+    for (uint32_t j0 = b; j0 < e; j0 += blockDim.x) {
+      const uint32_t j = j0 + threadIdx.x;
+      uint32_t mv = 0;
+      bool hit = false;
+      if (j < e) {
+        mv = g.col[j];
+        hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0) s_warp[wid] = __popc(bal);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < nw; ++k) {
+          const uint32_t x = s_warp[k];
+          s_warp[k] = run;
+          run += x;
+        }
+        s_total = run;
+      }
+      __syncthreads();
+      if (hit) nbrs[pos + s_warp[wid] + __popc(bal & ((1u << lane) - 1u))] = mv;
+      pos += s_total;
+      __syncthreads();
     }
   }
 }
@@ -323,39 +485,71 @@ void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t*
   GPSM_LAUNCHED();
 }
 
+static HeavyList heavy_list(Workspace& ws, const DeviceGraph& g) {
+  HeavyList hl;
+  hl.threshold = std::max<uint32_t>(tuning().heavy_degree, 32);
+  if (g.max_degree <= hl.threshold || ws.d_heavy == nullptr) return hl;
+  hl.items = ws.d_heavy;
+  hl.count = ws.d_heavy_count;
+  hl.cap = ws.heavy_cap;
+  GPSM_CUDA(cudaMemsetAsync(ws.d_heavy_count, 0, sizeof(uint32_t), ws.stream));
+  return hl;
+}
+
 void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
                     uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
   if (ntgt == 0 || max_count == 0) return;
+  HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(max_count, 148 * 16);
   k_explore<<<blocks, 256, 3 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm,
-                                                                    g.words, ws.d_flags);
+                                                                    g.words, ws.d_flags, hl);
   GPSM_LAUNCHED();
+  if (hl.items) {
+    k_explore_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags);
+    GPSM_LAUNCHED();
+  }
 }
 
 void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
                    uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
   if (ntgt == 0 || max_count == 0) return;
+  HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(max_count, 148 * 16);
   k_refine<<<blocks, 256, ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
-                                                               ws.d_flags);
+                                                               ws.d_flags, hl);
   GPSM_LAUNCHED();
+  if (hl.items) {
+    k_refine_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags);
+    GPSM_LAUNCHED();
+  }
 }
 
 void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
                         const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt) {
   if (items == 0) return;
+  HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(items, 148 * 16);
-  k_cedge_count<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, cnt);
+  k_cedge_count<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, cnt, hl);
   GPSM_LAUNCHED();
+  if (hl.items) {
+    k_cedge_count_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, cnt, hl);
+    GPSM_LAUNCHED();
+  }
 }
 
 void launch_cedge_write(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
                         const unsigned long long* d_base, uint64_t items, const uint32_t* bm,
                         const unsigned long long* goff, uint32_t* nbrs) {
   if (items == 0) return;
+  HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(items, 148 * 16);
-  k_cedge_write<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, goff, nbrs);
+  k_cedge_write<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, goff, nbrs, hl);
   GPSM_LAUNCHED();
+  if (hl.items) {
+    k_cedge_write_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, goff,
+                                                                nbrs, hl);
+    GPSM_LAUNCHED();
+  }
 }
 
 void launch_scan_u32(Workspace& ws, const uint32_t* in, uint64_t n, unsigned long long* out) {

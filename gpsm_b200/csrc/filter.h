@@ -14,6 +14,14 @@ struct GraphView {
 
 inline GraphView view(const DeviceGraph& g) { return GraphView{g.off, g.col, g.labdeg, g.n}; }
 
+// Candidates deferred by a warp kernel to a block-per-candidate kernel.
+struct HeavyList {
+  uint32_t* items = nullptr;
+  uint32_t* count = nullptr;
+  uint32_t cap = 0;
+  uint32_t threshold = 1024;  // degree above which a candidate is deferred
+};
+
 // One direction u->v of a query edge for candidate-edge collection.
 struct CedgeDir {
   const uint32_t* ids;           // final sorted candidate list of u

@@ -24,6 +24,21 @@
 
 namespace gpsm {
 
+static Tuning g_tuning;
+Tuning& tuning() { return g_tuning; }
+
+int sm_count() {
+  static int cached = 0;
+  if (cached == 0) {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0)
+      cached = n;
+    else
+      return 148;
+  }
+  return cached;
+}
+
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
@@ -165,6 +180,9 @@ Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) 
     GPSM_CUDA(cudaMalloc(&ws->d_flags, 64 * sizeof(uint32_t)));
     GPSM_CUDA(cudaMemset(ws->d_flags, 0, 64 * sizeof(uint32_t)));
     GPSM_CUDA(cudaMalloc(&ws->d_small, 4096 * sizeof(unsigned long long)));
+    ws->heavy_cap = 1u << 20;
+    GPSM_CUDA(cudaMalloc(&ws->d_heavy, ws->heavy_cap * sizeof(uint32_t)));
+    GPSM_CUDA(cudaMalloc(&ws->d_heavy_count, sizeof(uint32_t)));
     GPSM_CUDA(cudaMallocHost(&ws->h_small, 4096 * sizeof(unsigned long long)));
     GPSM_CUDA(cudaEventCreate(&ws->ev0));
     GPSM_CUDA(cudaEventCreate(&ws->evm));
@@ -181,6 +199,8 @@ Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) 
     cudaFree(ws->scan.d_status);
     cudaFree(ws->d_flags);
     cudaFree(ws->d_small);
+    cudaFree(ws->d_heavy);
+    cudaFree(ws->d_heavy_count);
     if (ws->h_small) cudaFreeHost(ws->h_small);
     delete ws;
     throw;
@@ -198,6 +218,8 @@ void workspace_free(Workspace* ws) {
   cudaFree(ws->scan.d_status);
   cudaFree(ws->d_flags);
   cudaFree(ws->d_small);
+  cudaFree(ws->d_heavy);
+  cudaFree(ws->d_heavy_count);
   cudaFreeHost(ws->h_small);
   cudaEventDestroy(ws->ev0);
   cudaEventDestroy(ws->evm);

@@ -88,6 +88,17 @@ struct ScanState {
   }
 };
 
+// Launch choices the autotuner may change (process-wide; read at each launch).
+struct Tuning {
+  uint32_t heavy_degree = 1024;    // candidates above it go to block-per-candidate kernels
+  uint32_t ext_blocks_per_sm = 8;  // persistent extend blocks per SM
+  uint64_t step_cands = 1ull << 25;  // candidates one join step may admit
+  uint64_t level_bytes = 256ull << 20;  // bytes per intermediate join level
+  uint32_t slots = 4;              // engine slots for batches and serving
+};
+Tuning& tuning();
+int sm_count();
+
 // bump allocator over one device allocation; reset per query
 struct Arena {
   char* base = nullptr;
@@ -116,6 +127,9 @@ struct Workspace {
   cudaEvent_t eve0 = nullptr, eve1 = nullptr;  // around each join launch
   cudaEvent_t evb0 = nullptr, evb1 = nullptr;  // around a batch
   bool dirty = false;  // a query stopped part-way; resynchronise scan tickets
+  uint32_t* d_heavy = nullptr;        // high-degree candidates handed to block-per-candidate kernels
+  uint32_t* d_heavy_count = nullptr;
+  uint32_t heavy_cap = 0;
 };
 
 }  // namespace gpsm

@@ -41,7 +41,9 @@ constexpr int kLocBlock = 256;  // rows per locate tile
 constexpr int kExtBlock = 256;
 constexpr int kExtItems = 4;
 constexpr int kExtTile = kExtBlock * kExtItems;  // candidates per extend tile
-constexpr uint32_t kExtGrid = 148 * 8;           // persistent extend blocks
+static uint32_t ext_grid() {  // persistent extend blocks
+  return (uint32_t)sm_count() * std::max<uint32_t>(1, std::min<uint32_t>(tuning().ext_blocks_per_sm, 8));
+}
 
 __device__ __forceinline__ bool sorted_contains(const uint32_t* __restrict__ a, unsigned long long lo,
                                                 unsigned long long hi, uint32_t key) {
@@ -344,9 +346,10 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   // candidates run out, then each takes one terminating ticket. The host
   // reserves the worst case; the kernel's last block moves the counter to
   // the end of the reservation.
-  const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + kExtGrid;
+  const uint32_t grid = ext_grid();
+  const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + grid;
   Lookback lb2 = next_lb(ws, reserved);
-  k_extend<<<kExtGrid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
+  k_extend<<<grid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
                                                   js.coff, out, out_cap, d_st, lb2, (unsigned long long)reserved);
   GPSM_LAUNCHED();
 }

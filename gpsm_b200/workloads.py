@@ -237,3 +237,37 @@ def read_text(path):
     if labels is not None:
         out.append((np.array(labels, np.uint32), np.array(edges, np.uint32).reshape(-1, 2)))
     return out
+
+
+def read_text_fast(path):
+    """read_text through libgpsm's parallel parser: [(labels, edges)]."""
+    import ctypes as C
+    lib = _lib.load()
+    h = _lib.vp()
+    _lib.check(lib.gpsm_text_open(path.encode(), C.byref(h)), "gpsm_text_open")
+    try:
+        k = C.c_uint32()
+        lib.gpsm_text_count(h, C.byref(k))
+        out = []
+        for i in range(k.value):
+            n, m, gid = C.c_uint32(), C.c_uint64(), C.c_int32()
+            _lib.check(lib.gpsm_text_graph_info(h, i, C.byref(n), C.byref(m), C.byref(gid)), "gpsm_text_graph_info")
+            lab = np.zeros(max(n.value, 1), np.uint32)
+            edg = np.zeros((max(m.value, 1), 2), np.uint32)
+            _lib.check(lib.gpsm_text_graph_read(h, i, _lib.ptr(lab), _lib.ptr(edg), None), "gpsm_text_graph_read")
+            out.append((lab[: n.value], edg[: m.value]))
+        return out
+    finally:
+        lib.gpsm_text_close(h)
+
+
+def write_text_fast(path, graphs, terminate=True):
+    """write_text through libgpsm's buffered writer."""
+    lib = _lib.load()
+    graphs = list(graphs)
+    for k, (labels, edges) in enumerate(graphs):
+        lab = _lib.u32a(labels)
+        edg = _lib.u32a(np.asarray(edges).reshape(-1))
+        _lib.check(lib.gpsm_text_write(path.encode(), 1 if k else 0, k, len(lab), _lib.ptr(lab), len(edg) // 2,
+                                       _lib.ptr(edg) if len(edg) else None, None,
+                                       1 if (terminate and k == len(graphs) - 1) else 0), "gpsm_text_write")

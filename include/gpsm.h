@@ -56,6 +56,25 @@ int64_t gpsm_gen_query(uint32_t n, const uint32_t* offsets, const uint32_t* cols
                        double min_avg_degree, uint64_t seed, uint32_t* q_labels,
                        uint32_t* q_edges, uint32_t* q_data_ids);
 
+/* ---- the reference's graph text format at full speed ------------------- */
+/* io/IO.cpp:87-142 reads `t # id`, a counts line, `v id label`, `e from to
+ * label`, ending with `t # -1`, one fscanf per token. These parse a whole
+ * file from a memory map with one thread per chunk of lines; vertices are
+ * numbered in file order (the `v` id is ignored, as Graph::addVertex does).
+ */
+typedef struct gpsm_text_s* gpsm_text_t;
+int gpsm_text_open(const char* path, gpsm_text_t* out);
+int gpsm_text_count(gpsm_text_t t, uint32_t* ngraphs);
+int gpsm_text_graph_info(gpsm_text_t t, uint32_t k, uint32_t* n, uint64_t* m, int32_t* id);
+/* labels[n]; edges[2m] (from, to) in file order; edge_labels[m] or NULL */
+int gpsm_text_graph_read(gpsm_text_t t, uint32_t k, uint32_t* labels, uint32_t* edges,
+                         uint32_t* edge_labels);
+int gpsm_text_close(gpsm_text_t t);
+/* Writes one graph (append != 0: after the file's contents); edge_labels
+ * NULL writes label 1; terminate != 0 adds the closing `t # -1`. */
+int gpsm_text_write(const char* path, int append, int32_t id, uint32_t n, const uint32_t* labels,
+                    uint64_t m, const uint32_t* edges, const uint32_t* edge_labels, int terminate);
+
 /* ---- engine: device, data graph, matching ------------------------------ */
 typedef struct gpsm_graph_s* gpsm_graph_t;   /* device-resident data graph */
 typedef struct gpsm_engine_s* gpsm_engine_t; /* stream + workspace on one device */
@@ -185,6 +204,42 @@ int gpsm_select_vertices(gpsm_engine_t e, const uint32_t* d_labels, const uint32
 int gpsm_select_vertices_static(const uint32_t* d_labels, const uint32_t* d_offsets, uint32_t n,
                                 uint32_t label, uint32_t min_degree, uint32_t* d_out,
                                 uint32_t* d_count, void* stream);
+/* The batch on `slots` engine slots of the graph's device (each its own
+ * stream and workspace of slot_arena bytes, 0 = automatic), each slot
+ * taking the next query when it finishes one, so queries overlap on the GPU.
+ * Same outputs as gpsm_match_batch; device time is the span from the first
+ * slot's start to the last slot's end. */
+int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_voff,
+                              const uint32_t* q_labels, const uint64_t* q_eoff,
+                              const uint32_t* q_edges, const gpsm_match_opts* opts,
+                              const int32_t* orders, uint32_t slots, uint64_t slot_arena,
+                              uint64_t* counts, int32_t* capped, double* query_ms,
+                              gpsm_batch_info* info);
+
+/* ---- serving: a request loop with memory admission ---------------------- */
+/* No counterpart in the reference (main/run.cpp matches queries one after
+ * another). Requests queue until a slot is free; the slot runs the filter
+ * and chooses the order, then the request waits until its predicted join
+ * memory fits memory_budget (0 = all slot workspaces) before joining. */
+typedef struct gpsm_server_s* gpsm_server_t;
+typedef struct gpsm_request_info {
+  int32_t status;          /* GPSM_OK or an error */
+  int32_t capped;
+  uint64_t rows;
+  double submit_ms, start_ms, admit_ms, end_ms;  /* server clock */
+  double device_ms;
+  uint64_t admitted_bytes;
+} gpsm_request_info;
+int gpsm_server_create(gpsm_graph_t g, uint32_t slots, uint64_t memory_budget, uint64_t slot_arena,
+                       const gpsm_match_opts* opts, int32_t collect_rows, gpsm_server_t* out);
+int gpsm_server_submit(gpsm_server_t s, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
+                       const uint32_t* q_edges, uint64_t* ticket);
+int gpsm_server_wait(gpsm_server_t s, uint64_t ticket, double timeout_s, gpsm_request_info* info,
+                     uint32_t** rows, int32_t* id_map);
+int gpsm_server_stats(gpsm_server_t s, uint64_t* in_use, uint64_t* peak_in_use, uint64_t* budget,
+                      uint32_t* queued, uint32_t* active);
+int gpsm_server_destroy(gpsm_server_t s);
+
 /* Writes `bytes` of device memory on the engine's stream (an L2 flush). */
 int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
 
@@ -193,6 +248,21 @@ int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
  * rows extended, candidates scanned, rows produced. */
 int gpsm_last_levels(gpsm_engine_t e, uint32_t n, uint64_t* level_in, uint64_t* level_cands,
                      uint64_t* level_out);
+
+/* ---- launch tuning (no counterpart in the reference) ------------------- */
+/* Process-wide launch choices; zero fields are left unchanged. The
+ * reference fixes its launch shapes in code (block sizes 32/256/1024,
+ * match/Match.cu:455, 649, 1313). */
+typedef struct gpsm_tuning {
+  uint32_t heavy_degree;       /* candidates with more neighbours: one block each (default 1024) */
+  uint32_t ext_blocks_per_sm;  /* persistent join-extend blocks per SM (1..8, default 8) */
+  uint64_t step_cands;         /* candidates one join step may admit (default 2^25) */
+  uint64_t level_bytes;        /* bytes per intermediate join level (default 256 MiB) */
+  uint32_t slots;              /* engine slots for batches and serving (default 4) */
+  uint32_t pad;
+} gpsm_tuning;
+int gpsm_set_tuning(const gpsm_tuning* t);
+int gpsm_get_tuning(gpsm_tuning* t);
 
 /* ---- learned join order (no counterpart in the reference) -------------- */
 /* 16 -> 64 -> 64 -> 1 MLP, BF16 weights, FP32 accumulation and masters.

@@ -1,0 +1,56 @@
+"""Multi-GPU is replicas only: each rank matches its own batch of the same
+shape against its own copy of the graph, and the bench takes the max of the
+ranks' step times and the sum of their work. The host side of that runs
+here as two gloo ranks on CPU."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import ROOT
+
+
+def _rank(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import bench
+    r, w, local, pg = bench.dist_setup(world)
+    assert (r, w) == (rank, world) and pg is not None
+    wl = bench.load_workload("small_er", rank)
+    bench.barrier(pg)
+    mx = bench.max_over_ranks(pg, 10.0 + rank)
+    sm = bench.sum_over_ranks(pg, len(wl.queries))
+    q.put((rank, mx, sm, [int(x) for x in wl.queries[0].labels], len(wl.queries)))
+    pg.destroy_process_group()
+
+
+def test_two_gloo_ranks_reduce_and_get_equal_sized_batches():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(2))
+    assert res[0][1] == res[1][1] == 11.0          # max over ranks
+    assert res[0][2] == res[1][2] == 20.0          # total work over ranks
+    assert res[0][4] == res[1][4]                  # same batch size per rank (weak scaling)
+
+
+def test_reference_arm_prints_one_json_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "small_er", "--steps", "1", "--warmup", "0", "--cpu-seconds", "2"],
+                         capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0

@@ -1,0 +1,60 @@
+"""Batched and served matching: same results whatever runs beside them."""
+import numpy as np
+import pytest
+
+from gpsm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mixed(gpu):
+    g = W.rmat_graph(14, 120000, 10, 1.0, seed=33)
+    qs = [W.random_walk_query(g, 4 + k % 6, 500 + k, W.MODE_DENSE if k % 2 else W.MODE_TREE, 0.4)
+          for k in range(24)]
+    return g, qs, gpu.DeviceGraph(g)
+
+
+def test_parallel_batch_equals_sequential(gpu, mixed):
+    g, qs, dg = mixed
+    c1, k1, _, i1 = gpu.match_batch(dg, qs, cap=200000)
+    c4, k4, _, i4 = gpu.match_batch(dg, qs, cap=200000, slots=4)
+    assert np.array_equal(c1, c4) and np.array_equal(k1, k4)
+    assert i4["rows"] == i1["rows"]
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(gpu, mixed):
+    g, qs, dg = mixed
+    srv = gpu.Server(dg, slots=4, cap=200000, collect_rows=True)
+    target = qs[5]
+    alone = srv.wait(srv.submit(target))
+    tickets = [srv.submit(q) for q in qs]  # 24 queries in flight on 4 slots
+    mid = srv.submit(target)
+    more = [srv.submit(q) for q in qs[:8]]
+    in_mix = srv.wait(mid)
+    rest = [srv.wait(t) for t in tickets + more]
+    srv.close()
+    assert alone["status"] == 0 and in_mix["status"] == 0
+    assert alone["rows"] == in_mix["rows"]
+    assert np.array_equal(alone["embeddings"], in_mix["embeddings"])
+    # and each query in the mix equals its own sequential run
+    for q, r in zip(qs, rest[: len(qs)]):
+        ref = gpu.match(dg, q, cap=200000)
+        assert r["rows"] == ref.count
+        assert np.array_equal(r["embeddings"], ref.embeddings())
+
+
+def test_admission_keeps_join_memory_within_budget(gpu, mixed):
+    g, qs, dg = mixed
+    budget = 3 << 30
+    srv = gpu.Server(dg, slots=4, memory_budget=budget, cap=100000, slot_arena=2 << 30)
+    ts = [srv.submit(q) for q in qs]
+    infos = [srv.wait(t) for t in ts]
+    st = srv.stats()
+    srv.close()
+    assert all(i["status"] == 0 for i in infos)
+    assert 0 < st["peak_in_use"] <= budget
+    assert all(i["admitted_bytes"] > 0 for i in infos if True)
+    # latencies are ordered: submit <= start <= admit <= end
+    for i in infos:
+        assert i["submit_ms"] <= i["start_ms"] <= i["admit_ms"] <= i["end_ms"]

@@ -63,20 +63,43 @@ def shutdown():
 
 
 class DeviceGraph:
-    """A data graph uploaded once to device memory (graph handle)."""
+    """A data graph uploaded once to device memory (graph handle).
+    build_on_device=True builds the CSR on the GPU from graph.edges."""
 
-    def __init__(self, graph):
+    def __init__(self, graph, build_on_device=False):
         lib = _lib.load()
         self._lib = lib
         self.graph = graph
         self.n = int(graph.n)
         h = _lib.vp()
-        off = _lib.u32a(graph.offsets)
-        cols = _lib.u32a(graph.cols) if len(graph.cols) else np.zeros(1, np.uint32)
         lab = _lib.u32a(graph.labels)
-        _lib.check(lib.gpsm_graph_upload(_lib.ptr(off), _lib.ptr(cols), _lib.ptr(lab), self.n, C.byref(h)),
-                   "gpsm_graph_upload")
+        if build_on_device:
+            e = _lib.u32a(np.asarray(graph.edges).reshape(-1))
+            _lib.check(lib.gpsm_graph_build(_lib.ptr(e), len(e) // 2, _lib.ptr(lab), self.n, C.byref(h)),
+                       "gpsm_graph_build")
+        else:
+            off = _lib.u32a(graph.offsets)
+            cols = _lib.u32a(graph.cols) if len(graph.cols) else np.zeros(1, np.uint32)
+            _lib.check(lib.gpsm_graph_upload(_lib.ptr(off), _lib.ptr(cols), _lib.ptr(lab), self.n, C.byref(h)),
+                       "gpsm_graph_upload")
         self.handle = h
+
+    def download(self):
+        """(offsets, cols) of the device CSR."""
+        nnz = C.c_uint64()
+        self._lib.gpsm_graph_info(self.handle, None, C.byref(nnz), None)
+        off = np.zeros(self.n + 1, np.uint32)
+        cols = np.zeros(max(nnz.value, 1), np.uint32)
+        _lib.check(self._lib.gpsm_graph_download(self.handle, _lib.ptr(off), _lib.ptr(cols)), "gpsm_graph_download")
+        return off, cols[: nnz.value]
+
+    def set_directed(self, edges, labels=None):
+        """Directed, labelled data edges (pairs (from, to) as in the file)
+        for directed matching (IO::verify's test on the device)."""
+        e = _lib.u32a(np.asarray(edges).reshape(-1))
+        lab = None if labels is None else _lib.u32a(labels)
+        _lib.check(self._lib.gpsm_graph_set_directed(self.handle, len(e) // 2, _lib.ptr(e), _lib.ptr(lab)),
+                   "gpsm_graph_set_directed")
 
     def free(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -138,7 +161,8 @@ def _query_arrays(query):
 
 
 def match(dgraph, query, cap=None, order=None, count_only=False, keep_on_device=False, engine=None,
-          level_bytes=0, result_rows=0, model=None, memory_budget=0, work_cap=0):
+          level_bytes=0, result_rows=0, model=None, memory_budget=0, work_cap=0, directed=False,
+          edge_labels=None):
     """Match one query (Match::match). order: None = the reference's plain
     join order, a pos2id list (a connected vertex order), or "learned" (the
     order chosen by `model`, falling back to the plain order when its
@@ -160,6 +184,12 @@ def match(dgraph, query, cap=None, order=None, count_only=False, keep_on_device=
         opts.order = order_arr.ctypes.data
     opts.memory_budget = int(memory_budget)
     opts.work_cap = int(work_cap)
+    elab = None
+    if directed:
+        opts.flags |= _lib.GPSM_F_DIRECTED
+        if edge_labels is not None:
+            elab = _lib.u32a(edge_labels)
+            opts.edge_labels = elab.ctypes.data
     opts.level_bytes = int(level_bytes)
     opts.result_rows = int(result_rows)
     opts.flags = (_lib.GPSM_F_COUNT_ONLY if count_only else 0) | (_lib.GPSM_F_KEEP_ON_DEVICE if keep_on_device else 0)

@@ -58,6 +58,9 @@ SIGNATURES = {
     "gpsm_graph_upload": (C.c_int, [vp, vp, vp, u32, vp]),
     "gpsm_graph_free": (C.c_int, [vp]),
     "gpsm_graph_info": (C.c_int, [vp, vp, vp, vp]),
+    "gpsm_graph_set_directed": (C.c_int, [vp, u64, vp, vp]),
+    "gpsm_graph_build": (C.c_int, [vp, u64, vp, u32, vp]),
+    "gpsm_graph_download": (C.c_int, [vp, vp, vp]),
     "gpsm_match_ex": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
     "gpsm_engine_match": (C.c_int, [vp, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
     "gpsm_match": (C.c_int, [vp, u32, vp, u32, vp, u64, vp, vp, vp, vp]),
@@ -88,13 +91,13 @@ SIGNATURES = {
 }
 
 GPSM_ORDER_PLAIN, GPSM_ORDER_GIVEN, GPSM_ORDER_LEARNED = 0, 1, 2
-GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE = 1, 2
+GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE, GPSM_F_DIRECTED = 1, 2, 4
 
 
 class MatchOpts(C.Structure):
     _fields_ = [("cap", u64), ("order_mode", i32), ("pad", i32), ("order", vp),
                 ("level_bytes", u64), ("result_rows", u64), ("flags", u32), ("pad2", u32),
-                ("model", vp), ("memory_budget", u64), ("work_cap", u64)]
+                ("model", vp), ("memory_budget", u64), ("work_cap", u64), ("edge_labels", vp)]
 
 
 class MatchInfo(C.Structure):

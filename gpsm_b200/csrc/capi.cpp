@@ -75,6 +75,7 @@ MatchOptions gpsm::options_from(const gpsm_match_opts* o) {
   }
   m.memory_budget = o->memory_budget;
   m.work_cap = o->work_cap;
+  m.directed = (o->flags & GPSM_F_DIRECTED) != 0;
   return m;
 }
 
@@ -205,6 +206,38 @@ int gpsm_graph_free(gpsm_graph_t g) {
   });
 }
 
+int gpsm_graph_build(const uint32_t* edges, uint64_t m, const uint32_t* labels, uint32_t n, gpsm_graph_t* out) {
+  if (!out) return GPSM_ERR_INVALID;
+  gpsm_engine_s* e = g_default;
+  if (!e) {
+    set_last_error("gpsm_init was not called");
+    return GPSM_ERR_STATE;
+  }
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(e->mu);
+    gpsm_graph_s* h = new gpsm_graph_s();
+    h->g = graph_build(*e->ws, edges, m, labels, n);
+    *out = h;
+    return GPSM_OK;
+  });
+}
+
+int gpsm_graph_download(gpsm_graph_t g, uint32_t* offsets, uint32_t* cols) {
+  if (!g) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    graph_download(g->g, offsets, cols);
+    return GPSM_OK;
+  });
+}
+
+int gpsm_graph_set_directed(gpsm_graph_t g, uint64_t m, const uint32_t* edges, const uint32_t* labels) {
+  if (!g || (m && !edges)) return GPSM_ERR_INVALID;
+  return guarded([&]() -> int {
+    graph_set_directed(g->g, m, edges, labels);
+    return GPSM_OK;
+  });
+}
+
 int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_degree) {
   if (!g) return GPSM_ERR_INVALID;
   if (n) *n = g->g->n;
@@ -240,6 +273,7 @@ int gpsm_engine_match(gpsm_engine_t eng, gpsm_graph_t g, uint32_t qn, const uint
       mo.given_order.assign(opts->order, opts->order + qn);
     }
     if (!out_rows) mo.collect_rows = false;
+    if (mo.directed && opts && opts->edge_labels) mo.edge_labels.assign(opts->edge_labels, opts->edge_labels + qm);
     if (mo.keep_on_device) mo.result_rows = std::max<uint64_t>(mo.result_rows, mo.cap == ~0ULL ? 0 : mo.cap);
     MatchResult R;
     rc = run_query(*e->ws, *g->g, Q, mo, R);

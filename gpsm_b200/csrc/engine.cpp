@@ -69,6 +69,8 @@ int plan_query(const DeviceGraph& g, uint32_t qn, const uint32_t* qlab, uint32_t
     seen.push_back(((uint64_t)std::min(a, b) << 32) | std::max(a, b));
     Q.out[a].push_back(b);
     Q.in[b].push_back(a);
+    Q.fe_from.push_back(a);
+    Q.fe_to.push_back(b);
   }
   std::sort(seen.begin(), seen.end());
   if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) {
@@ -666,6 +668,32 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
   if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
   uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
+  // directed mode: final rows land in a staging buffer and only those whose
+  // query edges are directed, labelled data edges move to the result
+  uint32_t* stage = nullptr;
+  uint64_t stage_rows = 0;
+  uint32_t* d_checks = nullptr;
+  unsigned long long* d_kept = nullptr;
+  uint32_t nchecks = 0;
+  if (opt.directed) {
+    if (!g.dir_off) {
+      set_last_error("directed mode needs gpsm_graph_set_directed");
+      return GPSM_ERR_STATE;
+    }
+    stage_rows = std::max<uint64_t>(opt.level_bytes / (4ull * qn), min_rows);
+    stage = arena_alloc<uint32_t>(ws, stage_rows * qn);
+    std::vector<uint32_t> chk;
+    for (uint32_t k = 0; k < Q.m; ++k) {  // every query edge a -> b (file order) with its label
+      chk.push_back((uint32_t)R.id2pos[Q.fe_from[k]]);
+      chk.push_back((uint32_t)R.id2pos[Q.fe_to[k]]);
+      chk.push_back(k < opt.edge_labels.size() ? opt.edge_labels[k] : 1u);
+    }
+    nchecks = (uint32_t)(chk.size() / 3);
+    d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
+    d_kept = arena_alloc<unsigned long long>(ws, 1);
+    if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+  }
   uint64_t res_used = 0, emitted = 0;
   bool capped = false;
 
@@ -719,7 +747,20 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     uint32_t* out;
     uint64_t out_cap, budget;
     bool partial = false;
-    if (final_level) {
+    if (final_level && opt.directed) {
+      uint64_t space = res_cap - res_used;
+      if (space == 0) {
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        flush();
+        space = res_cap;
+      }
+      out = stage;
+      out_cap = std::min<uint64_t>(stage_rows, space);
+      budget = std::min<uint64_t>(out_cap, opt.step_cands);
+    } else if (final_level) {
       uint64_t space = res_cap - res_used;
       out = res_buf + res_used * qn;
       if (cap - emitted <= space) {
@@ -780,6 +821,15 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
     A.next = rb + admitted;
     alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
+    uint64_t kept = written;
+    if (final_level && opt.directed && written) {
+      launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
+                             res_buf + res_used * qn, d_kept);
+      GPSM_CUDA(cudaMemcpyAsync(&h_st->pad, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      GPSM_CUDA(cudaStreamSynchronize(s));
+      kept = std::min<uint64_t>(h_st->pad, cap - emitted);  // the cap counts rows that pass
+      ++exp_launches;
+    }
     R.stats.level_rows[lv + 1] += written;
     R.stats.level_in[lv] += admitted;
     R.stats.level_cands[lv] += cands;
@@ -787,14 +837,14 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     if (opt.work_cap && cands_total >= opt.work_cap) {
       R.stats.aborted = true;
       if (final_level) {
-        res_used += written;
-        emitted += written;
+        res_used += kept;
+        emitted += kept;
       }
       break;
     }
     if (final_level) {
-      res_used += written;
-      emitted += written;
+      res_used += kept;
+      emitted += kept;
       if (emitted >= cap) capped = true;
     } else {
       L[lv + 1].nrows = written;

@@ -11,6 +11,14 @@ namespace gpsm {
 
 DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, const uint32_t* lab, uint32_t n);
 void graph_free(DeviceGraph* g);
+// CSR built on the device from m undirected edges (csr_build.cu); ws supplies scratch
+DeviceGraph* graph_build(Workspace& ws, const uint32_t* edges, uint64_t m, const uint32_t* lab, uint32_t n);
+void graph_download(const DeviceGraph* g, uint32_t* off, uint32_t* col);
+// attaches the directed, edge-labelled data edges (m pairs (from, to) + labels or NULL = 1)
+void graph_set_directed(DeviceGraph* g, uint64_t m, const uint32_t* edges, const uint32_t* labels);
+void launch_verify_directed(Workspace& ws, const uint32_t* in, uint64_t nrows, uint32_t cols, const uint32_t* d_checks,
+                            uint32_t nchecks, const uint32_t* off, const uint32_t* col, const uint32_t* lab,
+                            uint32_t* out, unsigned long long* d_kept);
 Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles);
 void workspace_free(Workspace* ws);
 
@@ -22,6 +30,7 @@ struct QueryPlan {
   std::vector<uint32_t> roff, rcol;             // undirected CSR, lists sorted (graph/Graph.cpp:190-226)
   std::vector<uint32_t> efrom, eto;             // edge ids (match/Match.cu:1738-1754), from < to
   std::vector<uint32_t> order;                  // filter order (match/Match.cu:339-429)
+  std::vector<uint32_t> fe_from, fe_to;         // edges as given (file order, directed)
   uint32_t deg(uint32_t u) const { return roff[u + 1] - roff[u]; }
   bool adjacent(uint32_t a, uint32_t b) const;
   int edge_between(uint32_t a, uint32_t b) const;  // edge id or -1
@@ -62,6 +71,8 @@ struct MatchOptions {
   bool collect_rows = true;             // false: count only (result rows are discarded)
   bool filter_only = false;             // stop after the join order (debug entry points)
   Model* model = nullptr;               // ORDER_LEARNED
+  bool directed = false;                // keep rows whose query edges exist as directed, labelled data edges
+  std::vector<uint32_t> edge_labels;    // per query edge in file order (empty = all 1)
   uint64_t memory_budget = 0;           // bytes; predicted peak above it -> plain order (0 = arena size)
   uint64_t work_cap = 0;                // candidates the joins may scan before stopping (0 = none)
   // Admission hook (serving): called after the order is chosen, before the

@@ -76,6 +76,84 @@ void DeviceGraph::label_range(uint32_t label, uint32_t d, uint32_t* begin, uint3
   *end = lo;
 }
 
+// Label index, derived arrays and bookkeeping for a graph whose offsets are
+// known on the host and whose CSR arrays are already on the device.
+static DeviceGraph* graph_finish(int device, uint32_t n, const uint32_t* off, const uint32_t* lab, uint32_t* d_off,
+                                 uint32_t* d_col) {
+  DeviceGraph* g = new DeviceGraph();
+  g->device = device;
+  g->n = n;
+  g->nnz = off[n];
+  g->words = (((n + 31) / 32) + 3) & ~3u;
+  g->off = d_off;
+  g->col = d_col;
+  uint32_t maxd = 0;
+  for (uint32_t i = 0; i < n; ++i) maxd = std::max(maxd, off[i + 1] - off[i]);
+  g->max_degree = maxd;
+  std::vector<uint32_t> idx(n);
+  std::iota(idx.begin(), idx.end(), 0u);
+  std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+    if (lab[a] != lab[b]) return lab[a] < lab[b];
+    uint32_t da = off[a + 1] - off[a], db = off[b + 1] - off[b];
+    if (da != db) return da > db;
+    return a < b;
+  });
+  g->h_lab_deg.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t x = idx[i];
+    g->h_lab_deg[i] = off[x + 1] - off[x];
+    if (i == 0 || lab[x] != lab[idx[i - 1]]) {
+      g->h_labels.push_back(lab[x]);
+      g->h_lab_ptr.push_back(i);
+    }
+  }
+  g->h_lab_ptr.push_back(n);
+  try {
+    GPSM_CUDA(cudaMalloc(&g->lab, sizeof(uint32_t) * n));
+    GPSM_CUDA(cudaMalloc(&g->labdeg, sizeof(uint2) * n));
+    GPSM_CUDA(cudaMalloc(&g->lab_vtx, sizeof(uint32_t) * n));
+    GPSM_CUDA(cudaMemcpy(g->lab, lab, sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    GPSM_CUDA(cudaMemcpy(g->lab_vtx, idx.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice));
+    k_labdeg<<<std::min<uint32_t>((n + 255) / 256, 148 * 8), 256>>>(g->off, g->lab, n, g->labdeg);
+    GPSM_LAUNCHED();
+    GPSM_CUDA(cudaDeviceSynchronize());
+  } catch (...) {
+    cudaFree(g->off);
+    cudaFree(g->col);
+    cudaFree(g->lab);
+    cudaFree(g->labdeg);
+    cudaFree(g->lab_vtx);
+    delete g;
+    throw;
+  }
+  return g;
+}
+
+void build_csr_device(Workspace& ws, uint32_t n, uint64_t m, const uint32_t* h_edges, uint32_t** d_off,
+                      uint32_t** d_cols);
+
+// CSR built on the device from an edge list (every undirected edge once).
+DeviceGraph* graph_build(Workspace& ws, const uint32_t* edges, uint64_t m, const uint32_t* lab, uint32_t n) {
+  if (n == 0 || lab == nullptr || (m && edges == nullptr)) throw CudaError{cudaErrorInvalidValue, "graph args"};
+  for (uint64_t i = 0; i < 2 * m; ++i)
+    if (edges[i] >= n) {
+      set_last_error("edge endpoint out of range");
+      throw CudaError{cudaErrorInvalidValue, "edges"};
+    }
+  GPSM_CUDA(cudaSetDevice(ws.device));
+  uint32_t *d_off = nullptr, *d_col = nullptr;
+  build_csr_device(ws, n, m, edges, &d_off, &d_col);
+  std::vector<uint32_t> off(n + 1);
+  GPSM_CUDA(cudaMemcpy(off.data(), d_off, (n + 1) * 4ull, cudaMemcpyDeviceToHost));
+  return graph_finish(ws.device, n, off.data(), lab, d_off, d_col);
+}
+
+void graph_download(const DeviceGraph* g, uint32_t* off, uint32_t* col) {
+  GPSM_CUDA(cudaSetDevice(g->device));
+  if (off) GPSM_CUDA(cudaMemcpy(off, g->off, (g->n + 1) * 4ull, cudaMemcpyDeviceToHost));
+  if (col && g->nnz) GPSM_CUDA(cudaMemcpy(col, g->col, g->nnz * 4ull, cudaMemcpyDeviceToHost));
+}
+
 DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, const uint32_t* lab, uint32_t n) {
   if (n == 0 || off == nullptr || lab == nullptr) throw CudaError{cudaErrorInvalidValue, "graph args"};
   const uint64_t nnz = off[n];
@@ -153,9 +231,55 @@ DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, 
   return g;
 }
 
+void graph_set_directed(DeviceGraph* g, uint64_t m, const uint32_t* edges, const uint32_t* labels) {
+  std::vector<uint32_t> off(g->n + 1, 0);
+  for (uint64_t i = 0; i < m; ++i) {
+    if (edges[2 * i] >= g->n || edges[2 * i + 1] >= g->n) {
+      set_last_error("directed edge endpoint out of range");
+      throw CudaError{cudaErrorInvalidValue, "directed edges"};
+    }
+    off[edges[2 * i] + 1]++;
+  }
+  for (uint32_t i = 0; i < g->n; ++i) off[i + 1] += off[i];
+  std::vector<uint64_t> key(m);  // (source, target, label) sorted: targets ascending per source
+  std::vector<uint32_t> pos(off.begin(), off.end() - 1);
+  std::vector<uint32_t> col(m), lab(m);
+  for (uint64_t i = 0; i < m; ++i) {
+    const uint32_t a = edges[2 * i];
+    const uint32_t k = pos[a]++;
+    col[k] = edges[2 * i + 1];
+    lab[k] = labels ? labels[i] : 1u;
+  }
+  for (uint32_t a = 0; a < g->n; ++a) {
+    std::vector<std::pair<uint32_t, uint32_t>> t;
+    for (uint32_t k = off[a]; k < off[a + 1]; ++k) t.emplace_back(col[k], lab[k]);
+    std::sort(t.begin(), t.end());
+    for (uint32_t k = off[a]; k < off[a + 1]; ++k) {
+      col[k] = t[k - off[a]].first;
+      lab[k] = t[k - off[a]].second;
+    }
+  }
+  GPSM_CUDA(cudaSetDevice(g->device));
+  cudaFree(g->dir_off);
+  cudaFree(g->dir_col);
+  cudaFree(g->dir_lab);
+  g->dir_off = g->dir_col = g->dir_lab = nullptr;
+  GPSM_CUDA(cudaMalloc(&g->dir_off, (g->n + 1) * 4));
+  GPSM_CUDA(cudaMalloc(&g->dir_col, std::max<uint64_t>(m, 1) * 4));
+  GPSM_CUDA(cudaMalloc(&g->dir_lab, std::max<uint64_t>(m, 1) * 4));
+  GPSM_CUDA(cudaMemcpy(g->dir_off, off.data(), (g->n + 1) * 4, cudaMemcpyHostToDevice));
+  if (m) {
+    GPSM_CUDA(cudaMemcpy(g->dir_col, col.data(), m * 4, cudaMemcpyHostToDevice));
+    GPSM_CUDA(cudaMemcpy(g->dir_lab, lab.data(), m * 4, cudaMemcpyHostToDevice));
+  }
+}
+
 void graph_free(DeviceGraph* g) {
   if (!g) return;
   cudaSetDevice(g->device);
+  cudaFree(g->dir_off);
+  cudaFree(g->dir_col);
+  cudaFree(g->dir_lab);
   cudaFree(g->off);
   cudaFree(g->col);
   cudaFree(g->lab);

@@ -60,6 +60,10 @@ struct DeviceGraph {
   std::vector<uint32_t> h_lab_ptr;  // [L+1] offsets into lab_vtx
   std::vector<uint32_t> h_lab_deg;  // [n] degrees in lab_vtx order (for cut-offs)
   uint32_t words = 0;               // bitmap words per candidate set (padded to 4)
+  // directed, edge-labelled data edges (optional): out-CSR sorted by (target, label)
+  uint32_t* dir_off = nullptr;
+  uint32_t* dir_col = nullptr;
+  uint32_t* dir_lab = nullptr;
   uint32_t max_degree = 0;
   // label frequency as the reference computes it (Graph::inverse_num)
   uint64_t label_count(uint32_t label) const;

@@ -92,6 +92,7 @@ def order_stats(dg, q, order, cap, model=None, work_cap=0):
     """Embeddings, join time and table sizes of one query under one order."""
     out = match(dg, q, cap=cap, order=order, model=model, count_only=True, work_cap=work_cap)
     lin, lc, lout = last_levels(q.n)
-    return dict(count=out.count, capped=out.capped, join_ms=out.info["join_ms"], device_ms=out.info["device_ms"],
+    return dict(count=out.count, capped=out.capped, aborted=bool(out.info["aborted"]), join_ms=out.info["join_ms"],
+                device_ms=out.info["device_ms"],
                 rows=int(lin[1:].sum()), cands=int(lc[1:].sum()), peak=int(lout[2:].max()) if q.n > 1 else 0,
                 pos2id=list(out.pos2id), fallback=bool(out.info["order_fallback"]))

@@ -100,7 +100,19 @@ int gpsm_engine_destroy(gpsm_engine_t e);
 int gpsm_graph_upload(const uint32_t* offsets, const uint32_t* cols, const uint32_t* labels,
                       uint32_t n, gpsm_graph_t* out);
 int gpsm_graph_free(gpsm_graph_t g);
+/* Builds the undirected CSR on the device from m undirected edges (pairs,
+ * each edge once) and labels[n]: Graph::transformToCSR's job
+ * (graph/Graph.cpp:190-226) done by a device radix sort. Same arrays as
+ * gpsm_csr_from_edges + gpsm_graph_upload. Scratch: the default engine. */
+int gpsm_graph_build(const uint32_t* edges, uint64_t m, const uint32_t* labels, uint32_t n,
+                     gpsm_graph_t* out);
+/* Copies a device graph's CSR back (offsets[n+1], cols[offsets[n]]; either may be NULL). */
+int gpsm_graph_download(gpsm_graph_t g, uint32_t* offsets, uint32_t* cols);
 int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_degree);
+/* Attaches the data graph's directed, edge-labelled edges (m pairs (from, to)
+ * as in the file, labels[m] or NULL = 1) for GPSM_F_DIRECTED. The reference
+ * keeps them in Graph::vertices[].out (graph/Graph.cpp:180-185). */
+int gpsm_graph_set_directed(gpsm_graph_t g, uint64_t m, const uint32_t* edges, const uint32_t* labels);
 
 #define GPSM_ORDER_PLAIN 0 /* the reference's join order (match/Match.cu:1599-1694) */
 #define GPSM_ORDER_GIVEN 1 /* opts.order gives the table columns (pos -> query vertex) */
@@ -110,6 +122,9 @@ typedef struct gpsm_model_s* gpsm_model_t; /* learned join-order model (MLP on o
 
 #define GPSM_F_COUNT_ONLY 1u      /* do not return rows (count and statistics only) */
 #define GPSM_F_KEEP_ON_DEVICE 2u  /* rows stay in device memory; never spill to host */
+#define GPSM_F_DIRECTED 4u        /* keep rows whose query edges a->b (label) are data edges
+                                     row[a]->row[b] with that label: IO::verify on the device
+                                     (io/IO.cpp:187-222); needs gpsm_graph_set_directed */
 
 typedef struct gpsm_match_opts {
   uint64_t cap;          /* embedding cap: stop after the first `cap` rows; 0 = none */
@@ -123,6 +138,7 @@ typedef struct gpsm_match_opts {
   gpsm_model_t model;    /* GPSM_ORDER_LEARNED */
   uint64_t memory_budget; /* bytes: predicted peak table above it -> plain order (0 = workspace size) */
   uint64_t work_cap;     /* candidates the joins may scan before the query stops (0 = none) */
+  const uint32_t* edge_labels; /* GPSM_F_DIRECTED: label per query edge (NULL = 1) */
 } gpsm_match_opts;
 
 typedef struct gpsm_match_info {

@@ -122,3 +122,8 @@ def pack():
 
 if __name__ == "__main__":
     {"inputs": inputs, "run": run, "pack": pack}[sys.argv[1]]()
+
+# small_er_ans.txt is the output file of the reference's own command line
+# driver (oracle/_ref/GpSM.exe, main/run.cpp) on small_er_{data,query}.g:
+#   oracle/_ref/GpSM.exe tests/golden/small_er_data.g tests/golden/small_er_query.g small_er_ans.txt 0
+# (rows after io/IO.cpp's directed, edge-labelled verify, in table order).

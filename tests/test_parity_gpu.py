@@ -200,3 +200,48 @@ def test_select_vertices_matches_label_degree_filter(gpu, lib):
         k = int(cnt.item())
         assert k == len(want)
         assert np.array_equal(out[:k].cpu().numpy().astype(np.int64), want)
+
+
+def test_directed_labelled_mode_equals_host_verify(gpu, small_er):
+    """GPSM_F_DIRECTED keeps exactly the rows io/IO.cpp:187-222 keeps: every
+    query edge a -> b (label l) must be a data edge row[a] -> row[b] with l."""
+    g = small_er.graph
+    rng = np.random.default_rng(3)
+    # data edges in both directions for half of the pairs, labels 1..2
+    flip = rng.random(g.m) < 0.5
+    e = g.edges.copy()
+    e[flip] = e[flip][:, ::-1]
+    both = rng.random(g.m) < 0.3
+    dir_edges = np.concatenate([e, e[both][:, ::-1]])
+    dir_labels = rng.integers(1, 3, size=len(dir_edges)).astype(np.uint32)
+    dg = gpu.DeviceGraph(g)
+    dg.set_directed(dir_edges, dir_labels)
+    have = {}
+    for (a, b), l in zip(dir_edges.tolist(), dir_labels.tolist()):
+        have.setdefault((a, b), set()).add(l)
+    for q in small_er.queries:
+        qe = np.asarray(q.edges)
+        ql = rng.integers(1, 3, size=len(qe)).astype(np.uint32)
+        rows, cnt = oracle.enumerate_embeddings(g, q)
+        want = [tuple(r) for r in rows.tolist()
+                if all(l in have.get((r[a], r[b]), ()) for (a, b), l in zip(qe.tolist(), ql.tolist()))]
+        out = gpu.match(dg, q, directed=True, edge_labels=ql)
+        assert _sorted_rows(out.embeddings()) == sorted(want)
+        # the cap counts rows that pass the directed test
+        if len(want) > 5:
+            capped = gpu.match(dg, q, directed=True, edge_labels=ql, cap=5)
+            full = gpu.match(dg, q, directed=True, edge_labels=ql)
+            assert capped.count == 5 and np.array_equal(capped.rows, full.rows[:5])
+
+
+@pytest.mark.parametrize("scale,m", [(10, 3000), (16, 400000)])
+def test_device_csr_build_equals_host_csr(gpu, scale, m):
+    g = W.rmat_graph(scale, m, 5, 1.0, seed=scale)
+    dg = gpu.DeviceGraph(g, build_on_device=True)
+    off, cols = dg.download()
+    assert np.array_equal(off, g.offsets) and np.array_equal(cols, g.cols)
+    # and matching on it gives the same rows as on the host-built graph
+    q = W.random_walk_query(g, 5, 9, W.MODE_DENSE, 0.5)
+    a = gpu.match(dg, q, cap=100000)
+    b = gpu.match(gpu.DeviceGraph(g), q, cap=100000)
+    assert np.array_equal(a.rows, b.rows)

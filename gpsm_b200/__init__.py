@@ -185,14 +185,13 @@ def match(dgraph, query, cap=None, order=None, count_only=False, keep_on_device=
     opts.memory_budget = int(memory_budget)
     opts.work_cap = int(work_cap)
     elab = None
-    if directed:
-        opts.flags |= _lib.GPSM_F_DIRECTED
-        if edge_labels is not None:
-            elab = _lib.u32a(edge_labels)
-            opts.edge_labels = elab.ctypes.data
+    if directed and edge_labels is not None:
+        elab = _lib.u32a(edge_labels)
+        opts.edge_labels = elab.ctypes.data
     opts.level_bytes = int(level_bytes)
     opts.result_rows = int(result_rows)
-    opts.flags = (_lib.GPSM_F_COUNT_ONLY if count_only else 0) | (_lib.GPSM_F_KEEP_ON_DEVICE if keep_on_device else 0)
+    opts.flags = ((_lib.GPSM_F_COUNT_ONLY if count_only else 0) | (_lib.GPSM_F_KEEP_ON_DEVICE if keep_on_device else 0)
+                  | (_lib.GPSM_F_DIRECTED if directed else 0))
     info = _lib.MatchInfo()
     id_map = np.zeros(qn, np.int32)
     pos2id = np.zeros(qn, np.int32)

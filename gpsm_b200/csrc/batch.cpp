@@ -37,10 +37,21 @@ struct SlotPool {
 static std::mutex g_pool_mu;
 static std::vector<SlotPool*> g_pools;
 
+uint64_t slot_arena_bytes(uint32_t slots, uint64_t per_slot) {
+  if (per_slot) return per_slot;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 2ull << 30;
+  return std::min<uint64_t>(16ull << 30, (uint64_t)(free_b * 0.5 / std::max<uint32_t>(slots, 1)));
+}
+
+// arena == 0: any existing pool of that many slots (its size was chosen from
+// the free memory when it was created; later calls must not size a second
+// pool from what the first one left free).
 SlotPool* slot_pool(int device, uint32_t slots, uint64_t arena) {
   std::lock_guard<std::mutex> lk(g_pool_mu);
   for (SlotPool* p : g_pools)
-    if (p->device == device && p->ws.size() == slots && p->arena == arena) return p;
+    if (p->device == device && p->ws.size() == slots && (arena == 0 || p->arena == arena)) return p;
+  if (arena == 0) arena = slot_arena_bytes(slots, 0);
   SlotPool* p = new SlotPool();
   p->device = device;
   p->arena = arena;
@@ -49,12 +60,6 @@ SlotPool* slot_pool(int device, uint32_t slots, uint64_t arena) {
   return p;
 }
 
-uint64_t slot_arena_bytes(uint32_t slots, uint64_t per_slot) {
-  if (per_slot) return per_slot;
-  size_t free_b = 0, total_b = 0;
-  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 2ull << 30;
-  return std::min<uint64_t>(16ull << 30, (uint64_t)(free_b * 0.5 / std::max<uint32_t>(slots, 1)));
-}
 
 struct BatchOut {
   std::vector<uint64_t> rows;
@@ -64,6 +69,7 @@ struct BatchOut {
   double device_ms = 0;
   uint64_t launches = 0, expand_launches = 0, alg_bytes = 0;
   double expand_ms = 0, filter_ms = 0;
+  std::string first_msg;  // error text of the first failing query (set on a worker thread)
 };
 
 // Runs queries [0, nq) on the pool's slots. Device time of the batch is the
@@ -116,11 +122,14 @@ int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const 
       out.status[k] = rc;
       if (rc != GPSM_OK) {
         int expected = GPSM_OK;
-        first_error.compare_exchange_strong(expected, rc);
+        if (first_error.compare_exchange_strong(expected, rc)) {
+          std::lock_guard<std::mutex> lk(agg_mu);
+          out.first_msg = "query " + std::to_string(k) + ": " + last_error();
+        }
         continue;
       }
       out.rows[k] = R.rows;
-      out.capped[k] = R.capped ? 1 : 0;
+      out.capped[k] = R.capped ? 1 : (R.stats.aborted ? 2 : 0);
       out.query_ms[k] = R.stats.device_ms;
       std::lock_guard<std::mutex> lk(agg_mu);
       out.launches += R.stats.filter_launches + R.stats.expand_launches;
@@ -286,10 +295,11 @@ int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_vof
     base.keep_on_device = true;
     base.collect_rows = false;
     if (base.cap != ~0ULL) base.result_rows = std::max<uint64_t>(base.result_rows, base.cap);
-    SlotPool* pool = slot_pool(g->g->device, slots, slot_arena_bytes(slots, slot_arena_bytes_in));
+    SlotPool* pool = slot_pool(g->g->device, slots, slot_arena_bytes_in);
     BatchOut out;
     int rc = run_batch_parallel(*pool, *g->g, nq, q_voff, q_labels, q_eoff, q_edges, base,
                                 (opts && opts->order_mode == GPSM_ORDER_GIVEN) ? orders : nullptr, out);
+    if (rc != GPSM_OK) set_last_error(out.first_msg);
     for (uint32_t k = 0; k < nq; ++k) {
       if (counts) counts[k] = out.rows[k];
       if (capped) capped[k] = out.capped[k];

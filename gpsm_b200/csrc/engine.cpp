@@ -268,7 +268,11 @@ bool trace_enabled() {
 template <class T>
 T* arena_alloc(Workspace& ws, uint64_t count) {
   void* p = ws.arena.alloc(std::max<uint64_t>(count, 1) * sizeof(T));
-  if (!p) throw CudaError{cudaErrorMemoryAllocation, "arena"};
+  if (!p) {
+    set_last_error("workspace arena exhausted: " + std::to_string(count * sizeof(T)) + " bytes requested, " +
+                   std::to_string(ws.arena.used) + " of " + std::to_string(ws.arena.size) + " in use");
+    throw CudaError{cudaErrorMemoryAllocation, "arena"};
+  }
   return (T*)p;
 }
 
@@ -332,24 +336,37 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   ws.arena.used = mark;  // planner scratch is not needed by the joins
   const size_t ob = plan_out_bytes();
   int best = -1;
-  float best_work = 0.f, best_peak = 0.f;
+  float best_work = 0.f;
   for (size_t i = 0; i < starts.size(); ++i) {
     const int32_t* order = reinterpret_cast<const int32_t*>(hout.data() + i * ob);
     const float work = *reinterpret_cast<const float*>(hout.data() + i * ob + kMaxPlanQ * 4);
-    const float peak = *reinterpret_cast<const float*>(hout.data() + i * ob + kMaxPlanQ * 4 + 4);
     std::vector<int32_t> ord(order, order + Q.n);
     if (!valid_order(Q, ord)) continue;
     if (best < 0 || work < best_work) {
       best = (int)i;
       best_work = work;
-      best_peak = peak;
+    }
+  }
+  if (best < 0) return {};
+  // predicted resident join memory: each width's table is held in chunks of
+  // at most one level buffer, the final rows in the result buffer
+  const float* logsz = reinterpret_cast<const float*>(hout.data() + (size_t)best * ob + kMaxPlanQ * 4 + 16);
+  const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+  double resident = 0;
+  for (uint32_t k = 1; k < Q.n; ++k) {  // position k holds tables of width k + 1
+    const uint32_t w = k + 1;
+    const double table = std::exp2((double)logsz[k]) * 4.0 * w;
+    if (w < Q.n) {
+      resident += std::min(table, (double)std::max<uint64_t>(opt.level_bytes, min_rows * 4ull * w));
+    } else {
+      const double res_rows = std::min<double>((double)std::max<uint64_t>(opt.result_rows, 1), (double)opt.cap);
+      resident += std::min(table, res_rows * 4.0 * w);
     }
   }
   st.predicted_work = best_work;
-  st.predicted_peak = best_peak;
-  if (best < 0) return {};
+  st.predicted_peak = resident;
   const uint64_t budget = opt.memory_budget ? opt.memory_budget : ws.arena.size;
-  if ((double)best_peak > (double)budget) {
+  if (resident > (double)budget) {
     st.order_fallback = true;
     return {};
   }
@@ -635,6 +652,18 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
   if (!hb.empty())
     GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
+  // per position: earlier columns holding a query vertex with the same label
+  std::vector<uint32_t> inj, inj_off(qn + 1, 0), inj_cnt(qn, 0);
+  for (uint32_t p = 1; p < qn; ++p) {
+    inj_off[p] = (uint32_t)inj.size();
+    for (uint32_t c = 0; c < p; ++c)
+      if (Q.lab[pos2id[c]] == Q.lab[pos2id[p]]) {
+        inj.push_back(c);
+        inj_cnt[p]++;
+      }
+  }
+  uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
+  if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
   StepState* d_st = arena_alloc<StepState>(ws, 1);
   StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
   JoinScratch js;
@@ -788,7 +817,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
     GPSM_CUDA(cudaEventRecord(ws.eve0, s));
     launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                     out_cap, js, d_st);
+                     out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 2;
     GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));

@@ -85,9 +85,11 @@ struct JoinScratch {
 // `budget`; admitted rows are extended by the query vertex whose placed
 // neighbours are back[0..nb) into `out` (in_cols+1 columns), at most out_cap
 // rows (the first out_cap in order). nbrs_total bounds every list range.
+// d_inj[0..ninj): the input columns whose query vertex has the new vertex's
+// label (the only columns a candidate can repeat).
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
-                      uint64_t out_cap, const JoinScratch& js, StepState* d_st);
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj);
 uint64_t join_rows_per_locate_tile();
 
 }  // namespace gpsm

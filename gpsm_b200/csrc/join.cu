@@ -140,6 +140,7 @@ constexpr uint32_t kSpan = 1024;  // rows of one tile whose offsets are staged i
 
 struct ExtendShared {
   BackNbr back[kMaxBack];
+  uint32_t inj[kMaxBack];  // columns whose query vertex has the new vertex's label
   uint32_t tile;
   unsigned long long prefix;
   unsigned long long r0, r1;  // rows holding the tile's first and last candidate
@@ -166,9 +167,11 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
                                                      const unsigned long long* __restrict__ coff,
                                                      uint32_t* __restrict__ out, unsigned long long out_cap,
                                                      StepState* __restrict__ st, Lookback lb,
-                                                     unsigned long long reserved) {
+                                                     unsigned long long reserved, const uint32_t* __restrict__ inj,
+                                                     uint32_t ninj) {
   __shared__ ExtendShared S;
   stage_back(S.back, back, nb);
+  for (uint32_t i = threadIdx.x; i < ninj; i += blockDim.x) S.inj[i] = inj[i];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const unsigned long long nr = st->rows;     // rows admitted by k_locate
   const unsigned long long ncand = nr ? coff[nr] : 0;
@@ -227,7 +230,9 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
       yv[k] = y;
       bool ok = !(kk > 0 && __ldg(nbrs + lo + kk - 1) == y);  // parallel data edges: once
       const uint32_t* row = in + (row_begin + r) * cols;
-      for (uint32_t c = 0; ok && c < cols; ++c) ok = __ldg(row + c) != y;
+      // a data vertex has one label, so y can only repeat a column whose
+      // query vertex has the new vertex's label
+      for (uint32_t c = 0; ok && c < ninj; ++c) ok = __ldg(row + S.inj[c]) != y;
       for (uint32_t j = 0; ok && j < nb; ++j) {
         if (j == d.w) continue;
         const uint4 g2 = __ldg(rng + r * nb + j);  // list of the row's j-th placed neighbour
@@ -330,7 +335,7 @@ uint64_t join_rows_per_locate_tile() { return kLocBlock; }
 
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
-                      uint64_t out_cap, const JoinScratch& js, StepState* d_st) {
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
   if (nrows > js.rows || nrows * nb > js.rng_entries) {
@@ -350,7 +355,8 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + grid;
   Lookback lb2 = next_lb(ws, reserved);
   k_extend<<<grid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
-                                                  js.coff, out, out_cap, d_st, lb2, (unsigned long long)reserved);
+                                                  js.coff, out, out_cap, d_st, lb2, (unsigned long long)reserved, d_inj,
+                                                  ninj);
   GPSM_LAUNCHED();
 }
 

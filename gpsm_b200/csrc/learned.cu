@@ -202,8 +202,9 @@ __global__ void k_mlp_to_bf16(const float* __restrict__ w, __nv_bfloat16* __rest
 struct PlanOut {
   int32_t order[kMaxPlanQ];
   float work;     // predicted sum_k 2^{L_k}
-  float peak;     // predicted max_k 2^{L_k} * 4 * (k + 1) bytes
+  float peak;     // predicted max_k 2^{L_k} * 4 * (k + 1) bytes (the largest whole table)
   float pad[2];
+  float logsize[kMaxPlanQ];  // L_k: predicted log2 rows of the table of width k + 1
 };
 
 __global__ void __launch_bounds__(256) k_plan(const PlanQuery* __restrict__ Qp, const PlanEdges* __restrict__ E,
@@ -223,6 +224,7 @@ __global__ void __launch_bounds__(256) k_plan(const PlanQuery* __restrict__ Qp, 
   P[v0 >> 6] |= 1ULL << (v0 & 63);
   if (lane == 0) O.order[0] = (int32_t)v0;
   float L = Q.log_cand[v0];
+  if (lane == 0) O.logsize[0] = L;
   float work = exp2f(L), peak = exp2f(L) * 4.f;
   for (uint32_t k = 1; k < n; ++k) {
     float best = 1e30f;
@@ -251,6 +253,7 @@ __global__ void __launch_bounds__(256) k_plan(const PlanQuery* __restrict__ Qp, 
     if (lane == 0) O.order[k] = (int32_t)bv;
     L += best;
     L = L < 0.f ? 0.f : L;
+    if (lane == 0) O.logsize[k] = L;
     const float rows = exp2f(L);
     work += rows;
     peak = fmaxf(peak, rows * 4.f * (float)(k + 1));

@@ -223,8 +223,9 @@ int gpsm_select_vertices_static(const uint32_t* d_labels, const uint32_t* d_offs
 /* The batch on `slots` engine slots of the graph's device (each its own
  * stream and workspace of slot_arena bytes, 0 = automatic), each slot
  * taking the next query when it finishes one, so queries overlap on the GPU.
- * Same outputs as gpsm_match_batch; device time is the span from the first
- * slot's start to the last slot's end. */
+ * Same outputs as gpsm_match_batch (capped[k] = 2 when opts->work_cap
+ * stopped query k); device time is the span from the first slot's start to
+ * the last slot's end. */
 int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_voff,
                               const uint32_t* q_labels, const uint64_t* q_eoff,
                               const uint32_t* q_edges, const gpsm_match_opts* opts,

@@ -245,7 +245,7 @@ def run_ours(args):
         tickets = [srv.submit(q) for q in wl.queries]
         for t in tickets:
             r = srv.wait(t)
-            d2h += r["embeddings"].nbytes
+            d2h += r["table"].nbytes
     e2e_wall = max_over_ranks(pg, time.perf_counter() - t1)
     srv.close()
     d2h //= e2e_steps

@@ -41,7 +41,7 @@ def init(device=0, arena_bytes=0, tuning_file=TUNING_FILE):
 
 def set_tuning(**kw):
     """Process-wide launch choices: heavy_degree, ext_blocks_per_sm,
-    step_cands, level_bytes, slots (unset or 0 = unchanged)."""
+    step_cands, level_bytes, slots, race_share (unset or 0 = unchanged)."""
     lib = _lib.load()
     t = _lib.Tuning()
     for k, v in kw.items():
@@ -203,15 +203,8 @@ def match(dgraph, query, cap=None, order=None, count_only=False, keep_on_device=
     _lib.check(rc, "gpsm_match")
     rows = None
     if not count_only:
-        nrows = int(info.rows)
-        if out.value:
-            buf = (C.c_uint32 * (nrows * qn)).from_address(out.value) if nrows * qn else None
-            rows = np.frombuffer(buf, dtype=np.uint32).copy().reshape(nrows, qn) if buf is not None else \
-                np.zeros((0, qn), np.uint32)
-            lib.gpsm_free(out)
-        else:
-            rows = np.zeros((0, qn), np.uint32)
-    d = {k: getattr(info, k) for k, _ in _lib.MatchInfo._fields_ if k not in ("pad",)}
+        rows = _lib.take_rows(lib, out.value, int(info.rows), qn)
+    d = {k: getattr(info, k) for k, _ in _lib.MatchInfo._fields_ if k not in ("pad", "pad2")}
     return MatchOutput(rows, int(info.rows), id_map, pos2id, bool(info.capped), bool(info.empty_filter), d)
 
 
@@ -416,17 +409,12 @@ class Server:
                                         C.byref(out) if self.collect else None, _lib.ptr(idm))
         _lib.check(rc, "gpsm_server_wait")
         d = {k: getattr(info, k) for k, _ in _lib.RequestInfo._fields_}
-        rows = None
         if self.collect:
-            n = int(info.rows)
-            if out.value and n:
-                buf = (C.c_uint32 * (n * qn)).from_address(out.value)
-                rows = np.frombuffer(buf, dtype=np.uint32).copy().reshape(n, qn)
-                self._lib.gpsm_free(out)
-            else:
-                rows = np.zeros((0, qn), np.uint32)
+            # the table in join-column order (as the reference returns it);
+            # column id_map[u] holds query vertex u: table[:, id_map] is the
+            # embeddings in query-vertex order
+            d["table"] = _lib.take_rows(self._lib, out.value, int(info.rows), qn)
             d["id_map"] = idm
-            d["embeddings"] = rows[:, idm] if len(rows) else rows
         return d
 
     def stats(self):

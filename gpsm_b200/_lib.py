@@ -105,12 +105,13 @@ class MatchInfo(C.Structure):
                 ("device_ms", f64), ("filter_ms", f64), ("join_ms", f64),
                 ("expand_launches", u64), ("filter_launches", u64), ("alg_bytes_join", u64),
                 ("expand_ms", f64), ("plan_ms", f64), ("predicted_work", f64), ("predicted_peak", f64),
-                ("order_fallback", i32), ("aborted", i32)]
+                ("order_fallback", i32), ("aborted", i32), ("predicted_work_plain", f64),
+                ("order_attempts", u32), ("pad2", u32), ("cands_scanned", u64)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", u32), ("ext_blocks_per_sm", u32), ("step_cands", u64), ("level_bytes", u64),
-                ("slots", u32), ("pad", u32)]
+                ("slots", u32), ("pad", u32), ("race_share", u64)]
 
 
 class RequestInfo(C.Structure):
@@ -161,3 +162,28 @@ def check(code, what):
 
 def u32a(x):
     return np.ascontiguousarray(x, dtype=np.uint32)
+
+
+class _Block:
+    """Frees one malloc'd result block of the library when collected."""
+
+    def __init__(self, lib, addr):
+        self.lib, self.addr = lib, addr
+
+    def __del__(self):
+        if self.addr:
+            self.lib.gpsm_free(C.c_void_p(self.addr))
+            self.addr = 0
+
+
+def take_rows(lib, addr, nrows, ncols):
+    """A (nrows, ncols) uint32 array over a result block the library handed
+    over (no copy); the block is freed with the last view of it."""
+    if not addr:
+        return np.zeros((0, ncols), np.uint32)
+    if nrows * ncols == 0:
+        lib.gpsm_free(C.c_void_p(addr))
+        return np.zeros((0, ncols), np.uint32)
+    buf = (C.c_uint32 * (nrows * ncols)).from_address(addr)
+    buf._owner = _Block(lib, addr)
+    return np.frombuffer(buf, dtype=np.uint32).reshape(nrows, ncols)

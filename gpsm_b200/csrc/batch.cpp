@@ -171,7 +171,7 @@ struct Request {
   int capped = 0;
   double device_ms = 0;
   uint64_t admitted_bytes = 0;
-  std::vector<uint32_t> result;  // rows (table-column order) when collect is on
+  HostRows result;  // rows (table-column order) when collect is on
   std::vector<int32_t> id2pos;
 };
 
@@ -396,13 +396,7 @@ int gpsm_server_wait(gpsm_server_t h, uint64_t ticket, double timeout_s, gpsm_re
     info->device_ms = r->device_ms;
     info->admitted_bytes = r->admitted_bytes;
   }
-  if (rows) {
-    *rows = nullptr;
-    if (!r->result.empty()) {
-      *rows = (uint32_t*)malloc(r->result.size() * 4);
-      if (*rows) memcpy(*rows, r->result.data(), r->result.size() * 4);
-    }
-  }
+  if (rows) *rows = r->result.empty() ? nullptr : r->result.release();  // the caller frees it
   if (id_map)
     for (uint32_t i = 0; i < r->qn; ++i) id_map[i] = i < r->id2pos.size() ? r->id2pos[i] : -1;
   const int st = r->status;

@@ -106,8 +106,11 @@ void fill_info(const MatchResult& R, gpsm_match_info* info) {
   info->plan_ms = R.stats.plan_ms;
   info->predicted_work = R.stats.predicted_work;
   info->predicted_peak = R.stats.predicted_peak;
-  info->order_fallback = R.stats.order_fallback ? 1 : 0;
+  info->order_fallback = R.stats.order_fallback;
   info->aborted = R.stats.aborted ? 1 : 0;
+  info->predicted_work_plain = R.stats.predicted_work_plain;
+  info->order_attempts = R.stats.order_attempts;
+  info->cands_scanned = R.stats.cands_scanned;
 }
 
 }  // namespace
@@ -284,20 +287,17 @@ int gpsm_engine_match(gpsm_engine_t eng, gpsm_graph_t g, uint32_t qn, const uint
       for (uint32_t i = 0; i < qn; ++i) pos2id[i] = R.pos2id.empty() ? -1 : R.pos2id[i];
     fill_info(R, info);
     if (out_rows && mo.collect_rows) {
-      const uint64_t words = R.rows * (uint64_t)qn;
-      uint32_t* buf = (uint32_t*)malloc(std::max<uint64_t>(words, 1) * sizeof(uint32_t));
+      // rows still on the device follow the flushed ones; the caller takes
+      // the host block itself
+      if (R.d_rows && R.d_rows_count)
+        copy_to_host(*e->ws, R.host_rows.append(R.d_rows_count * qn), R.d_rows, R.d_rows_count * qn);
+      R.d_rows = nullptr;
+      R.d_rows_count = 0;
+      uint32_t* buf = R.host_rows.release();
+      if (!buf) buf = (uint32_t*)malloc(sizeof(uint32_t));
       if (!buf) {
         set_last_error("host allocation of the result failed");
         return GPSM_ERR_NOMEM;
-      }
-      if (R.d_rows) {
-        const uint64_t hw = R.host_rows.size();
-        if (hw) memcpy(buf, R.host_rows.data(), hw * sizeof(uint32_t));
-        GPSM_CUDA(cudaMemcpyAsync(buf + hw, R.d_rows, R.d_rows_count * qn * sizeof(uint32_t),
-                                  cudaMemcpyDeviceToHost, e->ws->stream));
-        GPSM_CUDA(cudaStreamSynchronize(e->ws->stream));
-      } else if (words) {
-        memcpy(buf, R.host_rows.data(), words * sizeof(uint32_t));
       }
       *out_rows = buf;
     }
@@ -349,6 +349,7 @@ int gpsm_set_tuning(const gpsm_tuning* t) {
   if (t->step_cands) T.step_cands = std::max<uint64_t>(t->step_cands, 1u << 16);
   if (t->level_bytes) T.level_bytes = std::max<uint64_t>(t->level_bytes, 1u << 20);
   if (t->slots) T.slots = std::min<uint32_t>(t->slots, 64);
+  if (t->race_share) T.race_share = t->race_share;
   return GPSM_OK;
 }
 
@@ -360,6 +361,8 @@ int gpsm_get_tuning(gpsm_tuning* t) {
   t->step_cands = T.step_cands;
   t->level_bytes = T.level_bytes;
   t->slots = T.slots;
+  t->pad = 0;
+  t->race_share = T.race_share;
   return GPSM_OK;
 }
 

@@ -287,16 +287,24 @@ struct Level {
 }  // namespace
 
 void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const PlanEdges* d_e, const uint32_t* d_starts,
-                 uint32_t nstarts, void* d_out);
+                 uint32_t nstarts, const int32_t* d_fixed, void* d_out);
 size_t plan_out_bytes();
 
-// Learned order: greedy MLP plans from up to 8 start vertices on the device;
-// the plan with the smallest predicted work wins. Returns {} (plain order)
-// when its predicted peak table exceeds the memory budget.
+// A learned plan replaces the plain order only when the model predicts it
+// scans at most this fraction of the plain order's rows: the model's error
+// on one step is about 1.2 in log2 (validation MSE 1.49), so small predicted
+// gains are noise.
+constexpr double kLearnedMargin = 0.5;
+
+// Learned order: greedy MLP plans from up to 8 start vertices on the device,
+// scored with the plain order in the same launch; the plan with the smallest
+// predicted work wins if it beats the plain order by the margin. Returns {}
+// (plain order) otherwise, or when the plan's predicted resident join memory
+// exceeds the memory budget.
 static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q,
                                           const std::vector<uint32_t>& cnt, const std::vector<uint64_t>& size_fwd,
-                                          const std::vector<uint64_t>& size_rev, const MatchOptions& opt,
-                                          MatchStats& st) {
+                                          const std::vector<uint64_t>& size_rev, const std::vector<int32_t>& plain,
+                                          const MatchOptions& opt, MatchStats& st) {
   static thread_local std::unique_ptr<PlanQuery> PQ(new PlanQuery());
   static thread_local std::unique_ptr<PlanEdges> PE(new PlanEdges());
   build_plan_inputs(g, Q, cnt, size_fwd, size_rev, *PQ, *PE);
@@ -323,14 +331,16 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   PlanQuery* d_q = arena_alloc<PlanQuery>(ws, 1);
   PlanEdges* d_e = arena_alloc<PlanEdges>(ws, 1);
   uint32_t* d_st = arena_alloc<uint32_t>(ws, 8);
-  char* d_out = arena_alloc<char>(ws, plan_out_bytes() * 8);
+  int32_t* d_fixed = arena_alloc<int32_t>(ws, kMaxPlanQ);
+  char* d_out = arena_alloc<char>(ws, plan_out_bytes() * 9);
   cudaStream_t s = ws.stream;
   GPSM_CUDA(cudaMemcpyAsync(d_q, PQ.get(), sizeof(PlanQuery), cudaMemcpyHostToDevice, s));
   // only the rows of the n query vertices matter; copy the whole table for simplicity
   GPSM_CUDA(cudaMemcpyAsync(d_e, PE.get(), sizeof(PlanEdges), cudaMemcpyHostToDevice, s));
   GPSM_CUDA(cudaMemcpyAsync(d_st, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
-  launch_plan(s, opt.model, d_q, d_e, d_st, (uint32_t)starts.size(), d_out);
-  std::vector<char> hout(plan_out_bytes() * starts.size());
+  GPSM_CUDA(cudaMemcpyAsync(d_fixed, plain.data(), Q.n * 4, cudaMemcpyHostToDevice, s));
+  launch_plan(s, opt.model, d_q, d_e, d_st, (uint32_t)starts.size(), d_fixed, d_out);
+  std::vector<char> hout(plan_out_bytes() * (starts.size() + 1));
   GPSM_CUDA(cudaMemcpyAsync(hout.data(), d_out, hout.size(), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaStreamSynchronize(s));
   ws.arena.used = mark;  // planner scratch is not needed by the joins
@@ -347,6 +357,9 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
       best_work = work;
     }
   }
+  const float plain_work =
+      *reinterpret_cast<const float*>(hout.data() + starts.size() * ob + kMaxPlanQ * 4);
+  st.predicted_work_plain = plain_work;
   if (best < 0) return {};
   // predicted resident join memory: each width's table is held in chunks of
   // at most one level buffer, the final rows in the result buffer
@@ -367,7 +380,11 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   st.predicted_peak = resident;
   const uint64_t budget = opt.memory_budget ? opt.memory_budget : ws.arena.size;
   if (resident > (double)budget) {
-    st.order_fallback = true;
+    st.order_fallback = 1;
+    return {};
+  }
+  if ((double)best_work > kLearnedMargin * (double)plain_work) {
+    st.order_fallback = 2;
     return {};
   }
   const int32_t* order = reinterpret_cast<const int32_t*>(hout.data() + (size_t)best * ob);
@@ -569,6 +586,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
 
   // ---- join order -------------------------------------------------------------
   std::vector<int32_t> pos2id;
+  std::vector<int32_t> race;  // the plain order, when a learned plan runs against it
   if (opt.order_mode == ORDER_GIVEN) {
     if (!valid_order(Q, opt.given_order)) {
       set_last_error("given join order is not a connected permutation of the query vertices");
@@ -581,8 +599,10 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       return GPSM_ERR_INVALID;
     }
     const auto tp0 = std::chrono::steady_clock::now();
-    pos2id = learned_order(ws, g, Q, cnt, R.stats.size_fwd, R.stats.size_rev, opt, R.stats);
-    if (pos2id.empty()) pos2id = plain_order(Q, R.stats.size_fwd, g.nnz);
+    const std::vector<int32_t> plain = plain_order(Q, R.stats.size_fwd, g.nnz);
+    pos2id = learned_order(ws, g, Q, cnt, R.stats.size_fwd, R.stats.size_rev, plain, opt, R.stats);
+    if (pos2id.empty()) pos2id = plain;
+    else if (pos2id != plain) race = plain;
     R.stats.plan_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count();
   } else {
     pos2id = plain_order(Q, R.stats.size_fwd, g.nnz);
@@ -627,270 +647,312 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   }
 
   // ---- joins ---------------------------------------------------------------------
-  // back-neighbour descriptors for each added position p >= 1
-  std::vector<BackNbr> hb;
-  std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
-  for (uint32_t p = 1; p < qn; ++p) {
-    back_off[p] = (uint32_t)hb.size();
-    const uint32_t v = (uint32_t)pos2id[p];
-    for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
-      const uint32_t w = Q.rcol[k];
-      if ((uint32_t)R.id2pos[w] >= p) continue;
-      const int e = Q.edge_between(w, v);
-      const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
-      BackNbr b;
-      b.col = (uint32_t)R.id2pos[w];
-      b.pad = 0;
-      b.bm = bm_of(w);
-      b.rank = rank + (size_t)w * W;
-      b.off = goff + dirs[d].item_base;
-      b.nbrs = nbrs;
-      hb.push_back(b);
-      back_cnt[p]++;
-    }
-  }
-  BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
-  if (!hb.empty())
-    GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
-  // per position: earlier columns holding a query vertex with the same label
-  std::vector<uint32_t> inj, inj_off(qn + 1, 0), inj_cnt(qn, 0);
-  for (uint32_t p = 1; p < qn; ++p) {
-    inj_off[p] = (uint32_t)inj.size();
-    for (uint32_t c = 0; c < p; ++c)
-      if (Q.lab[pos2id[c]] == Q.lab[pos2id[p]]) {
-        inj.push_back(c);
-        inj_cnt[p]++;
+  // One attempt joins in the order pos2id until the embeddings are complete,
+  // the cap is reached or `limit` candidates have been scanned (limit 0: no
+  // limit); hit_limit reports the last. Every attempt starts from the same
+  // filter products: it takes join memory from join_mark on and resets the
+  // result state.
+  const size_t join_mark = ws.arena.used;
+  uint64_t exp_launches = 0;  // over all attempts
+  uint64_t alg_bytes = 0;
+  auto join_attempt = [&](uint64_t limit, bool& hit_limit) -> int {
+    hit_limit = false;
+    ws.arena.used = join_mark;
+    R.pos2id = pos2id;
+    R.id2pos.assign(qn, -1);
+    for (uint32_t p = 0; p < qn; ++p) R.id2pos[pos2id[p]] = (int32_t)p;
+    R.host_rows.clear();
+    R.d_rows = nullptr;
+    R.d_rows_count = 0;
+    // back-neighbour descriptors for each added position p >= 1
+    std::vector<BackNbr> hb;
+    std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
+    for (uint32_t p = 1; p < qn; ++p) {
+      back_off[p] = (uint32_t)hb.size();
+      const uint32_t v = (uint32_t)pos2id[p];
+      for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
+        const uint32_t w = Q.rcol[k];
+        if ((uint32_t)R.id2pos[w] >= p) continue;
+        const int e = Q.edge_between(w, v);
+        const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
+        BackNbr b;
+        b.col = (uint32_t)R.id2pos[w];
+        b.pad = 0;
+        b.bm = bm_of(w);
+        b.rank = rank + (size_t)w * W;
+        b.off = goff + dirs[d].item_base;
+        b.nbrs = nbrs;
+        hb.push_back(b);
+        back_cnt[p]++;
       }
-  }
-  uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
-  if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
-  StepState* d_st = arena_alloc<StepState>(ws, 1);
-  StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
-  JoinScratch js;
-  uint32_t max_nb = 1;
-  for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
-  // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
-  js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
-  js.rng_entries = js.rows * max_nb;
-  js.drv = arena_alloc<uint4>(ws, js.rows);
-  js.rng = arena_alloc<uint4>(ws, js.rng_entries);
-  js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
-  GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
-
-  R.stats.level_rows.assign(qn + 1, 0);
-  R.stats.level_in.assign(qn + 1, 0);
-  R.stats.level_cands.assign(qn + 1, 0);
-  uint64_t cands_total = 0;
-  const uint64_t cap = opt.cap;
-  // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
-  std::vector<Level> L(qn + 1);
-  L[1].buf = list[pos2id[0]];
-  L[1].nrows = cnt[pos2id[0]];
-  L[1].cap_rows = L[1].nrows;
-  R.stats.level_rows[1] = L[1].nrows;
-  const uint64_t min_rows = (uint64_t)g.max_degree + 64;
-  for (uint32_t w = 2; w < qn; ++w) {
-    uint64_t rows = std::max<uint64_t>(opt.level_bytes / (4ull * w), min_rows);
-    L[w].cap_rows = rows;
-    L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
-  }
-  uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
-  if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
-  uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
-  // directed mode: final rows land in a staging buffer and only those whose
-  // query edges are directed, labelled data edges move to the result
-  uint32_t* stage = nullptr;
-  uint64_t stage_rows = 0;
-  uint32_t* d_checks = nullptr;
-  unsigned long long* d_kept = nullptr;
-  uint32_t nchecks = 0;
-  if (opt.directed) {
-    if (!g.dir_off) {
-      set_last_error("directed mode needs gpsm_graph_set_directed");
-      return GPSM_ERR_STATE;
     }
-    stage_rows = std::max<uint64_t>(opt.level_bytes / (4ull * qn), min_rows);
-    stage = arena_alloc<uint32_t>(ws, stage_rows * qn);
-    std::vector<uint32_t> chk;
-    for (uint32_t k = 0; k < Q.m; ++k) {  // every query edge a -> b (file order) with its label
-      chk.push_back((uint32_t)R.id2pos[Q.fe_from[k]]);
-      chk.push_back((uint32_t)R.id2pos[Q.fe_to[k]]);
-      chk.push_back(k < opt.edge_labels.size() ? opt.edge_labels[k] : 1u);
+    BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
+    if (!hb.empty())
+      GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
+    // per position: earlier columns holding a query vertex with the same label
+    std::vector<uint32_t> inj, inj_off(qn + 1, 0), inj_cnt(qn, 0);
+    for (uint32_t p = 1; p < qn; ++p) {
+      inj_off[p] = (uint32_t)inj.size();
+      for (uint32_t c = 0; c < p; ++c)
+        if (Q.lab[pos2id[c]] == Q.lab[pos2id[p]]) {
+          inj.push_back(c);
+          inj_cnt[p]++;
+        }
     }
-    nchecks = (uint32_t)(chk.size() / 3);
-    d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
-    d_kept = arena_alloc<unsigned long long>(ws, 1);
-    if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
-    GPSM_CUDA(cudaStreamSynchronize(s));
-  }
-  uint64_t res_used = 0, emitted = 0;
-  bool capped = false;
+    uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
+    if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
+    StepState* d_st = arena_alloc<StepState>(ws, 1);
+    StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
+    JoinScratch js;
+    uint32_t max_nb = 1;
+    for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
+    // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
+    js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
+    js.rng_entries = js.rows * max_nb;
+    js.drv = arena_alloc<uint4>(ws, js.rows);
+    js.rng = arena_alloc<uint4>(ws, js.rng_entries);
+    js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
+    GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
-  auto flush = [&]() {
-    if (!opt.collect_rows || res_used == 0) {
+    R.stats.level_rows.assign(qn + 1, 0);
+    R.stats.level_in.assign(qn + 1, 0);
+    R.stats.level_cands.assign(qn + 1, 0);
+    uint64_t cands_total = 0;
+    const uint64_t cap = opt.cap;
+    // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
+    std::vector<Level> L(qn + 1);
+    L[1].buf = list[pos2id[0]];
+    L[1].nrows = cnt[pos2id[0]];
+    L[1].cap_rows = L[1].nrows;
+    R.stats.level_rows[1] = L[1].nrows;
+    const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+    for (uint32_t w = 2; w < qn; ++w) {
+      uint64_t rows = std::max<uint64_t>(opt.level_bytes / (4ull * w), min_rows);
+      L[w].cap_rows = rows;
+      L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
+    }
+    uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
+    if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
+    uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
+    // directed mode: final rows land in a staging buffer and only those whose
+    // query edges are directed, labelled data edges move to the result
+    uint32_t* stage = nullptr;
+    uint64_t stage_rows = 0;
+    uint32_t* d_checks = nullptr;
+    unsigned long long* d_kept = nullptr;
+    uint32_t nchecks = 0;
+    if (opt.directed) {
+      if (!g.dir_off) {
+        set_last_error("directed mode needs gpsm_graph_set_directed");
+        return GPSM_ERR_STATE;
+      }
+      stage_rows = std::max<uint64_t>(opt.level_bytes / (4ull * qn), min_rows);
+      stage = arena_alloc<uint32_t>(ws, stage_rows * qn);
+      std::vector<uint32_t> chk;
+      for (uint32_t k = 0; k < Q.m; ++k) {  // every query edge a -> b (file order) with its label
+        chk.push_back((uint32_t)R.id2pos[Q.fe_from[k]]);
+        chk.push_back((uint32_t)R.id2pos[Q.fe_to[k]]);
+        chk.push_back(k < opt.edge_labels.size() ? opt.edge_labels[k] : 1u);
+      }
+      nchecks = (uint32_t)(chk.size() / 3);
+      d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
+      d_kept = arena_alloc<unsigned long long>(ws, 1);
+      if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
+      GPSM_CUDA(cudaStreamSynchronize(s));
+    }
+    uint64_t res_used = 0, emitted = 0;
+    bool capped = false;
+
+    auto flush = [&]() {
+      if (!opt.collect_rows || res_used == 0) {
+        res_used = 0;
+        return;
+      }
+      copy_to_host(ws, R.host_rows.append(res_used * qn), res_buf, res_used * qn);
       res_used = 0;
-      return;
-    }
-    size_t old = R.host_rows.size();
-    R.host_rows.resize(old + res_used * qn);
-    GPSM_CUDA(cudaMemcpyAsync(R.host_rows.data() + old, res_buf, res_used * qn * 4, cudaMemcpyDeviceToHost, s));
-    GPSM_CUDA(cudaStreamSynchronize(s));
-    res_used = 0;
-  };
+    };
 
-  if (qn == 1) {
-    // single-vertex query: every candidate is an embedding
-    const uint64_t n1 = std::min<uint64_t>(L[1].nrows, cap);
-    capped = L[1].nrows >= cap;
-    if (n1 > 0)
-      GPSM_CUDA(cudaMemcpyAsync(res_buf, L[1].buf, std::min(n1, res_cap) * 4, cudaMemcpyDeviceToDevice, s));
-    if (n1 > res_cap) {
-      if (opt.keep_on_device) {
-        set_last_error("device result buffer full");
+    if (qn == 1) {
+      // single-vertex query: every candidate is an embedding
+      const uint64_t n1 = std::min<uint64_t>(L[1].nrows, cap);
+      capped = L[1].nrows >= cap;
+      if (n1 > 0)
+        GPSM_CUDA(cudaMemcpyAsync(res_buf, L[1].buf, std::min(n1, res_cap) * 4, cudaMemcpyDeviceToDevice, s));
+      if (n1 > res_cap) {
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        if (opt.collect_rows) {
+          R.host_rows.clear();
+          copy_to_host(ws, R.host_rows.append(n1), L[1].buf, n1);
+        }
+      } else {
+        res_used = n1;
+      }
+      emitted = n1;
+      R.stats.level_rows[1] = n1;
+    }
+    while (qn > 1 && !capped) {
+      // deepest level with rows left
+      int lv = -1;
+      for (int w = (int)qn - 1; w >= 1; --w)
+        if (L[w].next < L[w].nrows) {
+          lv = w;
+          break;
+        }
+      if (lv < 0) break;
+      Level& A = L[lv];
+      const bool final_level = (uint32_t)lv + 1 == qn;
+      uint32_t* out;
+      uint64_t out_cap, budget;
+      bool partial = false;
+      if (final_level && opt.directed) {
+        uint64_t space = res_cap - res_used;
+        if (space == 0) {
+          if (opt.keep_on_device) {
+            set_last_error("device result buffer full");
+            return GPSM_ERR_BUDGET;
+          }
+          flush();
+          space = res_cap;
+        }
+        out = stage;
+        out_cap = std::min<uint64_t>(stage_rows, space);
+        budget = std::min<uint64_t>(out_cap, opt.step_cands);
+      } else if (final_level) {
+        uint64_t space = res_cap - res_used;
+        out = res_buf + res_used * qn;
+        if (cap - emitted <= space) {
+          // the cap ends the query inside this buffer: rows past it are cut
+          out_cap = cap - emitted;
+          partial = true;
+          budget = std::min<uint64_t>(std::max<uint64_t>(out_cap, min_rows), opt.step_cands);
+        } else {
+          out_cap = space;
+          budget = std::min<uint64_t>(space, opt.step_cands);
+        }
+      } else {
+        Level& B = L[lv + 1];
+        B.nrows = 0;
+        B.next = 0;
+        out = B.buf;
+        out_cap = B.cap_rows;
+        budget = std::min<uint64_t>(out_cap, opt.step_cands);
+      }
+      // rows offered to this step: enough to fill the budget at the observed
+      // candidates per row, within the per-row scratch
+      uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
+      want = std::min<uint64_t>(want, js.rows);
+      const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
+      GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
+      GPSM_CUDA(cudaEventRecord(ws.eve0, s));
+      launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
+                       out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
+      GPSM_CUDA(cudaEventRecord(ws.eve1, s));
+      exp_launches += 2;
+      GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
+      GPSM_CUDA(cudaStreamSynchronize(s));
+      {
+        float ems = 0;
+        GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
+        R.stats.expand_ms += ems;
+      }
+      const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
+      if (trace_enabled()) {
+        float ems = 0;
+        cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
+        fprintf(stderr, "[gpsm] step level=%d rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu ms=%.3f\n",
+                lv, (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
+                (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ems);
+      }
+      if (admitted == 0) {
+        if (final_level && !partial && res_used > 0) {  // make room and retry
+          if (opt.keep_on_device) {
+            set_last_error("device result buffer full");
+            return GPSM_ERR_BUDGET;
+          }
+          flush();
+          continue;
+        }
+        set_last_error("a single row has more candidates than a join step admits");
         return GPSM_ERR_BUDGET;
       }
-      if (opt.collect_rows) {
-        R.host_rows.resize(n1);
-        GPSM_CUDA(cudaMemcpyAsync(R.host_rows.data(), L[1].buf, n1 * 4, cudaMemcpyDeviceToHost, s));
+      A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
+      A.next = rb + admitted;
+      alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
+      uint64_t kept = written;
+      if (final_level && opt.directed && written) {
+        launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
+                               res_buf + res_used * qn, d_kept);
+        GPSM_CUDA(cudaMemcpyAsync(&h_st->pad, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         GPSM_CUDA(cudaStreamSynchronize(s));
+        kept = std::min<uint64_t>(h_st->pad, cap - emitted);  // the cap counts rows that pass
+        ++exp_launches;
       }
-    } else {
-      res_used = n1;
-    }
-    emitted = n1;
-    R.stats.level_rows[1] = n1;
-  }
-  uint64_t exp_launches = 0;
-  uint64_t alg_bytes = 0;
-  while (qn > 1 && !capped) {
-    // deepest level with rows left
-    int lv = -1;
-    for (int w = (int)qn - 1; w >= 1; --w)
-      if (L[w].next < L[w].nrows) {
-        lv = w;
+      R.stats.level_rows[lv + 1] += written;
+      R.stats.level_in[lv] += admitted;
+      R.stats.level_cands[lv] += cands;
+      cands_total += cands;
+      R.stats.cands_scanned += cands;
+      if (limit && cands_total >= limit) {
+        hit_limit = true;
+        if (final_level) {
+          res_used += kept;
+          emitted += kept;
+        }
         break;
       }
-    if (lv < 0) break;
-    Level& A = L[lv];
-    const bool final_level = (uint32_t)lv + 1 == qn;
-    uint32_t* out;
-    uint64_t out_cap, budget;
-    bool partial = false;
-    if (final_level && opt.directed) {
-      uint64_t space = res_cap - res_used;
-      if (space == 0) {
-        if (opt.keep_on_device) {
-          set_last_error("device result buffer full");
-          return GPSM_ERR_BUDGET;
-        }
-        flush();
-        space = res_cap;
-      }
-      out = stage;
-      out_cap = std::min<uint64_t>(stage_rows, space);
-      budget = std::min<uint64_t>(out_cap, opt.step_cands);
-    } else if (final_level) {
-      uint64_t space = res_cap - res_used;
-      out = res_buf + res_used * qn;
-      if (cap - emitted <= space) {
-        // the cap ends the query inside this buffer: rows past it are cut
-        out_cap = cap - emitted;
-        partial = true;
-        budget = std::min<uint64_t>(std::max<uint64_t>(out_cap, min_rows), opt.step_cands);
-      } else {
-        out_cap = space;
-        budget = std::min<uint64_t>(space, opt.step_cands);
-      }
-    } else {
-      Level& B = L[lv + 1];
-      B.nrows = 0;
-      B.next = 0;
-      out = B.buf;
-      out_cap = B.cap_rows;
-      budget = std::min<uint64_t>(out_cap, opt.step_cands);
-    }
-    // rows offered to this step: enough to fill the budget at the observed
-    // candidates per row, within the per-row scratch
-    uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
-    want = std::min<uint64_t>(want, js.rows);
-    const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
-    GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
-    GPSM_CUDA(cudaEventRecord(ws.eve0, s));
-    launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                     out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
-    GPSM_CUDA(cudaEventRecord(ws.eve1, s));
-    exp_launches += 2;
-    GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
-    GPSM_CUDA(cudaStreamSynchronize(s));
-    {
-      float ems = 0;
-      GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
-      R.stats.expand_ms += ems;
-    }
-    const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
-    if (trace_enabled()) {
-      float ems = 0;
-      cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
-      fprintf(stderr, "[gpsm] step level=%d rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu ms=%.3f\n",
-              lv, (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
-              (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ems);
-    }
-    if (admitted == 0) {
-      if (final_level && !partial && res_used > 0) {  // make room and retry
-        if (opt.keep_on_device) {
-          set_last_error("device result buffer full");
-          return GPSM_ERR_BUDGET;
-        }
-        flush();
-        continue;
-      }
-      set_last_error("a single row has more candidates than a join step admits");
-      return GPSM_ERR_BUDGET;
-    }
-    A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
-    A.next = rb + admitted;
-    alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
-    uint64_t kept = written;
-    if (final_level && opt.directed && written) {
-      launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
-                             res_buf + res_used * qn, d_kept);
-      GPSM_CUDA(cudaMemcpyAsync(&h_st->pad, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-      GPSM_CUDA(cudaStreamSynchronize(s));
-      kept = std::min<uint64_t>(h_st->pad, cap - emitted);  // the cap counts rows that pass
-      ++exp_launches;
-    }
-    R.stats.level_rows[lv + 1] += written;
-    R.stats.level_in[lv] += admitted;
-    R.stats.level_cands[lv] += cands;
-    cands_total += cands;
-    if (opt.work_cap && cands_total >= opt.work_cap) {
-      R.stats.aborted = true;
       if (final_level) {
         res_used += kept;
         emitted += kept;
+        if (emitted >= cap) capped = true;
+      } else {
+        L[lv + 1].nrows = written;
       }
-      break;
     }
-    if (final_level) {
-      res_used += kept;
-      emitted += kept;
-      if (emitted >= cap) capped = true;
+    if (emitted >= cap) capped = true;
+    R.rows = emitted;
+    R.capped = capped;
+    GPSM_CUDA(cudaEventRecord(ws.ev1, s));
+    if (opt.collect_rows && !opt.keep_on_device) {
+      flush();
     } else {
-      L[lv + 1].nrows = written;
+      R.d_rows = res_buf;
+      R.d_rows_count = res_used;
+    }
+    return GPSM_OK;
+  };
+
+  int jrc = GPSM_OK;
+  bool hit = false;
+  if (race.empty()) {
+    jrc = join_attempt(opt.work_cap, hit);
+    R.stats.aborted = hit;
+  } else {
+    // the learned plan and the plain order take turns with work shares that
+    // grow by 4 each round, until one finishes; the total work stays within
+    // a small factor of the cheaper order's, so a plan the model got wrong
+    // costs a bounded share instead of its whole blowup
+    const std::vector<int32_t> learned_plan = pos2id;
+    uint64_t share = tuning().race_share;
+    for (uint32_t a = 0;; ++a) {
+      const bool learned_turn = (a % 2) == 0;
+      pos2id = learned_turn ? learned_plan : race;
+      const bool last = (opt.work_cap && share >= opt.work_cap) || share >= (1ull << 60);
+      ++R.stats.order_attempts;
+      jrc = join_attempt(last ? opt.work_cap : share, hit);
+      if (jrc != GPSM_OK || !hit || last) {
+        R.stats.aborted = hit;
+        if (!learned_turn) R.stats.order_fallback = 3;
+        break;
+      }
+      if (!learned_turn) share *= 4;
     }
   }
-  if (emitted >= cap) capped = true;
   R.stats.expand_launches = exp_launches;
   R.stats.alg_bytes_join = alg_bytes;
-  R.rows = emitted;
-  R.capped = capped;
-  GPSM_CUDA(cudaEventRecord(ws.ev1, s));
-  if (opt.collect_rows && !opt.keep_on_device) {
-    flush();
-  } else {
-    R.d_rows = res_buf;
-    R.d_rows_count = res_used;
-  }
+  if (jrc != GPSM_OK) return jrc;
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4001, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaEventSynchronize(ws.ev1));
   GPSM_CUDA(cudaStreamSynchronize(s));

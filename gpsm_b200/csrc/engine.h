@@ -97,10 +97,50 @@ struct MatchStats {
   double expand_ms = 0;         // summed device time of the join launches
   double plan_ms = 0;           // learned-order planning (host wall time incl. the planner kernel)
   double predicted_work = 0, predicted_peak = 0;
-  bool order_fallback = false;  // learned order rejected by the memory budget
+  double predicted_work_plain = 0;  // the model's work estimate for the plain order
+  int order_fallback = 0;  // 1: learned order over the memory budget; 2: not predicted cheaper than plain;
+                           // 3: raced the plain order, which finished first
+  uint32_t order_attempts = 0;  // join attempts when a learned plan raced the plain order
+  uint64_t cands_scanned = 0;   // candidates the joins scanned, over all attempts
   uint64_t admitted_bytes = 0;  // bytes granted by the admission hook
   bool aborted = false;         // work cap reached
   uint64_t alg_bytes_filter = 0;
+};
+
+// Result rows on the host: one malloc'd block (a caller can take it with
+// release() and free() it), grown with realloc and never zero-filled; large
+// blocks ask for transparent huge pages, so first touch of a 10^7-row result
+// costs a fault per 2 MiB instead of per 4 KiB.
+class HostRows {
+ public:
+  HostRows() = default;
+  HostRows(const HostRows&) = delete;
+  HostRows& operator=(const HostRows&) = delete;
+  HostRows(HostRows&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_) { o.p_ = nullptr, o.n_ = o.cap_ = 0; }
+  HostRows& operator=(HostRows&& o) noexcept {
+    if (this != &o) {
+      free(p_);
+      p_ = o.p_, n_ = o.n_, cap_ = o.cap_;
+      o.p_ = nullptr, o.n_ = o.cap_ = 0;
+    }
+    return *this;
+  }
+  ~HostRows() { free(p_); }
+  uint64_t size() const { return n_; }  // words
+  bool empty() const { return n_ == 0; }
+  const uint32_t* data() const { return p_; }
+  void clear() { n_ = 0; }
+  // room for `words` more words at the end; the size grows by that much
+  uint32_t* append(uint64_t words);
+  uint32_t* release() {
+    uint32_t* q = p_;
+    p_ = nullptr, n_ = cap_ = 0;
+    return q;
+  }
+
+ private:
+  uint32_t* p_ = nullptr;
+  uint64_t n_ = 0, cap_ = 0;
 };
 
 struct MatchResult {
@@ -109,7 +149,7 @@ struct MatchResult {
   bool capped = false;
   bool empty_filter = false;        // a candidate set ran empty (no embeddings)
   std::vector<int32_t> id2pos, pos2id;
-  std::vector<uint32_t> host_rows;  // flushed rows (row-major, table column order)
+  HostRows host_rows;               // flushed rows (row-major, table column order)
   uint32_t* d_rows = nullptr;       // rows still on the device (arena memory; valid until the next query)
   uint64_t d_rows_count = 0;        // rows in d_rows (after host_rows)
   MatchStats stats;

@@ -345,6 +345,10 @@ void workspace_free(Workspace* ws) {
   cudaFree(ws->d_heavy);
   cudaFree(ws->d_heavy_count);
   cudaFreeHost(ws->h_small);
+  for (int i = 0; i < 2; ++i) {
+    if (ws->h_stage[i]) cudaFreeHost(ws->h_stage[i]);
+    if (ws->ev_stage[i]) cudaEventDestroy(ws->ev_stage[i]);
+  }
   cudaEventDestroy(ws->ev0);
   cudaEventDestroy(ws->evm);
   cudaEventDestroy(ws->eve0);

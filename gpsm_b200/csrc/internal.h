@@ -99,6 +99,10 @@ struct Tuning {
   uint64_t step_cands = 1ull << 25;  // candidates one join step may admit
   uint64_t level_bytes = 256ull << 20;  // bytes per intermediate join level
   uint32_t slots = 4;              // engine slots for batches and serving
+  // first work share (candidates scanned) of a learned plan racing the plain
+  // order: about 20 ms of joins on one B200, enough for a capped query of
+  // 10^7 embeddings in a good order
+  uint64_t race_share = 1ull << 28;
 };
 Tuning& tuning();
 int sm_count();
@@ -134,6 +138,17 @@ struct Workspace {
   uint32_t* d_heavy = nullptr;        // high-degree candidates handed to block-per-candidate kernels
   uint32_t* d_heavy_count = nullptr;
   uint32_t heavy_cap = 0;
+  // two pinned staging buffers for result rows on their way to the host
+  // (allocated at the first copy): the DMA fills one while the host thread
+  // moves the other into the caller's buffer
+  static constexpr size_t kStageBytes = 32ull << 20;
+  void* h_stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
 };
+
+// Copies `words` 32-bit words from device memory to pageable host memory
+// through the workspace's pinned staging buffers, on the workspace stream;
+// returns when dst holds them.
+void copy_to_host(Workspace& ws, uint32_t* dst, const uint32_t* d_src, uint64_t words);
 
 }  // namespace gpsm

@@ -207,20 +207,24 @@ struct PlanOut {
   float logsize[kMaxPlanQ];  // L_k: predicted log2 rows of the table of width k + 1
 };
 
-__global__ void __launch_bounds__(256) k_plan(const PlanQuery* __restrict__ Qp, const PlanEdges* __restrict__ E,
+// One warp per start vertex builds a greedy order; when `fixed` is given,
+// warp `nstarts` scores that order instead (same predictions, no choice).
+__global__ void __launch_bounds__(288) k_plan(const PlanQuery* __restrict__ Qp, const PlanEdges* __restrict__ E,
                                               const uint32_t* __restrict__ starts, uint32_t nstarts,
+                                              const int32_t* __restrict__ fixed,
                                               const __nv_bfloat16* __restrict__ wb, const float* __restrict__ wf,
                                               PlanOut* __restrict__ outs) {
   __shared__ MlpSmem S;
   stage_weights(S, wb, wf);
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (wid >= nstarts) return;
+  const bool follow = fixed && wid == nstarts;
+  if (wid >= nstarts && !follow) return;
   const PlanQuery& Q = *Qp;
   const uint32_t n = Q.n;
   PlanOut& O = outs[wid];
   uint64_t P[2] = {0, 0};
-  const uint32_t v0 = starts[wid];
+  const uint32_t v0 = follow ? (uint32_t)fixed[0] : starts[wid];
   P[v0 >> 6] |= 1ULL << (v0 & 63);
   if (lane == 0) O.order[0] = (int32_t)v0;
   float L = Q.log_cand[v0];
@@ -232,6 +236,7 @@ __global__ void __launch_bounds__(256) k_plan(const PlanQuery* __restrict__ Qp, 
     for (uint32_t v = lane; v < n; v += 32) {
       if (pq_has(P, v)) continue;
       if (!((Q.adj[v][0] & P[0]) | (Q.adj[v][1] & P[1]))) continue;
+      if (follow && v != (uint32_t)fixed[k]) continue;
       float x[kFeat], h1[kHidden], h2[kHidden];
       step_features(Q, *E, P, k, v, x);
       const float d = mlp_eval(S, x, h1, h2);
@@ -426,10 +431,13 @@ void model_predict(Model* M, const float* x, uint32_t n, float* y) {
 
 // Runs the planner for `nstarts` start vertices on `stream`; d_q, d_e, d_starts
 // and d_out are device buffers (workspace memory). Asynchronous.
+// d_fixed (or null): an order of the n query vertices to score; its result
+// is written after the nstarts greedy plans.
 void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const PlanEdges* d_e, const uint32_t* d_starts,
-                 uint32_t nstarts, void* d_out) {
-  k_plan<<<1, 32 * std::max<uint32_t>(1, std::min<uint32_t>(nstarts, 8)), 0, s>>>(d_q, d_e, d_starts, nstarts, M->wb,
-                                                                                   M->w, (PlanOut*)d_out);
+                 uint32_t nstarts, const int32_t* d_fixed, void* d_out) {
+  nstarts = std::min<uint32_t>(nstarts, 8);
+  const uint32_t warps = std::max<uint32_t>(1, nstarts + (d_fixed ? 1 : 0));
+  k_plan<<<1, 32 * warps, 0, s>>>(d_q, d_e, d_starts, nstarts, d_fixed, M->wb, M->w, (PlanOut*)d_out);
   GPSM_LAUNCHED();
 }
 

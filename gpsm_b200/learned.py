@@ -94,5 +94,8 @@ def order_stats(dg, q, order, cap, model=None, work_cap=0):
     lin, lc, lout = last_levels(q.n)
     return dict(count=out.count, capped=out.capped, aborted=bool(out.info["aborted"]), join_ms=out.info["join_ms"],
                 device_ms=out.info["device_ms"],
-                rows=int(lin[1:].sum()), cands=int(lc[1:].sum()), peak=int(lout[2:].max()) if q.n > 1 else 0,
-                pos2id=[int(x) for x in out.pos2id], fallback=bool(out.info["order_fallback"]))
+                rows=int(lin[1:].sum()), cands=int(out.info["cands_scanned"]), peak=int(lout[2:].max()) if q.n > 1 else 0,
+                pos2id=[int(x) for x in out.pos2id], fallback=int(out.info["order_fallback"]),
+                predicted_work=float(out.info["predicted_work"]),
+                predicted_work_plain=float(out.info["predicted_work_plain"]),
+                attempts=int(out.info["order_attempts"]))

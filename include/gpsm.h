@@ -157,8 +157,15 @@ typedef struct gpsm_match_info {
   double plan_ms;            /* learned-order planning */
   double predicted_work;     /* learned order: predicted sum of table sizes */
   double predicted_peak;     /* learned order: predicted peak table bytes */
-  int32_t order_fallback;    /* 1: learned order over the memory budget, plain order used */
+  int32_t order_fallback;    /* plain order used instead of the learned plan: 1 its predicted join memory is
+                                over the budget; 2 it is not predicted to scan under half the plain order's rows;
+                                3 the two orders took turns with growing work shares and the plain order
+                                finished first */
   int32_t aborted;           /* 1: work_cap stopped the joins (rows are a prefix) */
+  double predicted_work_plain; /* learned order: the model's predicted work of the plain order */
+  uint32_t order_attempts;   /* learned order: join attempts of the two orders (0: no race) */
+  uint32_t pad2;
+  uint64_t cands_scanned;    /* candidates the joins scanned, over all attempts */
 } gpsm_match_info;
 
 typedef struct gpsm_batch_info {
@@ -277,6 +284,8 @@ typedef struct gpsm_tuning {
   uint64_t level_bytes;        /* bytes per intermediate join level (default 256 MiB) */
   uint32_t slots;              /* engine slots for batches and serving (default 4) */
   uint32_t pad;
+  uint64_t race_share;         /* learned order: first work share (candidates) when the learned plan
+                                  and the plain order take turns (default 2^28) */
 } gpsm_tuning;
 int gpsm_set_tuning(const gpsm_tuning* t);
 int gpsm_get_tuning(gpsm_tuning* t);

@@ -81,6 +81,31 @@ def test_memory_budget_falls_back_to_plain_order(gpu, small_er, small_dg):
     assert np.array_equal(out.rows, plain.rows)
 
 
+def test_race_restarts_return_the_finishing_orders_rows(gpu):
+    """A learned plan takes turns with the plain order under growing work
+    shares; whichever order finishes, the rows are exactly those of a match
+    in that order (restarts leave nothing behind)."""
+    from gpsm_b200 import learned as L
+    model = L.load(0) if os.path.exists(L.WEIGHTS) else gpu.Model(0, seed=4)
+    g = W.rmat_graph(12, 24000, 12, 1.0, seed=5)
+    dg = gpu.DeviceGraph(g)
+    old = gpu.get_tuning()
+    gpu.set_tuning(race_share=2048)
+    raced = 0
+    try:
+        for k in range(40):
+            q = W.random_walk_query(g, 6 + k % 4, 300 + k, W.MODE_DENSE if k % 2 else W.MODE_TREE, 0.5)
+            for cap in (200_000, 5000):
+                out = gpu.match(dg, q, cap=cap, order="learned", model=model)
+                ref = gpu.match(dg, q, cap=cap, order=list(out.pos2id))
+                assert out.count == ref.count
+                assert np.array_equal(out.embeddings(), ref.embeddings())
+                raced += out.info["order_attempts"] >= 2
+    finally:
+        gpu.set_tuning(race_share=old["race_share"])
+    assert raced > 0
+
+
 def test_trained_model_reduces_join_work(gpu):
     from gpsm_b200 import learned as L
     if not os.path.exists(L.WEIGHTS):

@@ -291,10 +291,11 @@ int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_vof
                               int32_t* capped, double* query_ms, gpsm_batch_info* info) {
   if (!g || !q_voff || !q_labels || !q_eoff || slots == 0 || slots > 64) return GPSM_ERR_INVALID;
   try {
+    // counts only: final rows are produced on the device and dropped once
+    // counted, so the result buffer holds one step's output, not the cap
     MatchOptions base = options_from(opts);
-    base.keep_on_device = true;
+    base.keep_on_device = false;
     base.collect_rows = false;
-    if (base.cap != ~0ULL) base.result_rows = std::max<uint64_t>(base.result_rows, base.cap);
     SlotPool* pool = slot_pool(g->g->device, slots, slot_arena_bytes_in);
     BatchOut out;
     int rc = run_batch_parallel(*pool, *g->g, nq, q_voff, q_labels, q_eoff, q_edges, base,

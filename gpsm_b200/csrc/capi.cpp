@@ -476,10 +476,10 @@ int gpsm_match_batch(gpsm_engine_t eng, gpsm_graph_t g, uint32_t nq, const uint3
   return guarded([&]() -> int {
     std::lock_guard<std::mutex> lk(e->mu);
     Workspace& ws = *e->ws;
+    // counts only: final rows are dropped on the device once counted
     MatchOptions base = to_options(opts);
-    base.keep_on_device = true;
+    base.keep_on_device = false;
     base.collect_rows = false;
-    if (base.cap != ~0ULL) base.result_rows = std::max<uint64_t>(base.result_rows, base.cap);
     gpsm_batch_info bi;
     memset(&bi, 0, sizeof(bi));
     GPSM_CUDA(cudaEventRecord(ws.evb0, ws.stream));
@@ -502,7 +502,7 @@ int gpsm_match_batch(gpsm_engine_t eng, gpsm_graph_t g, uint32_t nq, const uint3
       rc = run_query(ws, *g->g, Q, mo, R);
       if (rc != GPSM_OK) return rc;
       if (counts) counts[k] = R.rows;
-      if (capped) capped[k] = R.capped ? 1 : 0;
+      if (capped) capped[k] = R.capped ? 1 : (R.stats.aborted ? 2 : 0);
       if (query_ms) query_ms[k] = R.stats.device_ms;
       bi.rows += R.rows;
       bi.launches += R.stats.filter_launches + R.stats.expand_launches;

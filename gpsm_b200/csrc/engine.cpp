@@ -290,6 +290,16 @@ void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const Pla
                  uint32_t nstarts, const int32_t* d_fixed, void* d_out);
 size_t plan_out_bytes();
 
+// Bytes of one intermediate level buffer: the configured size, shrunk for
+// deep queries so that the n - 2 level buffers together take at most half
+// of the workspace arena (a 64-vertex query would otherwise ask for 62 full
+// buffers).
+static uint64_t level_buffer_bytes(const Workspace& ws, const MatchOptions& opt, uint32_t qn) {
+  uint64_t lb = opt.level_bytes;
+  if (qn > 2) lb = std::min<uint64_t>(lb, (ws.arena.size / 2) / (qn - 2));
+  return std::max<uint64_t>(lb, 1ull << 20);
+}
+
 // A learned plan replaces the plain order only when the model predicts it
 // scans at most this fraction of the plain order's rows: the model's error
 // on one step is about 1.2 in log2 (validation MSE 1.49), so small predicted
@@ -365,12 +375,13 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   // at most one level buffer, the final rows in the result buffer
   const float* logsz = reinterpret_cast<const float*>(hout.data() + (size_t)best * ob + kMaxPlanQ * 4 + 16);
   const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+  const uint64_t lb = level_buffer_bytes(ws, opt, Q.n);
   double resident = 0;
   for (uint32_t k = 1; k < Q.n; ++k) {  // position k holds tables of width k + 1
     const uint32_t w = k + 1;
     const double table = std::exp2((double)logsz[k]) * 4.0 * w;
     if (w < Q.n) {
-      resident += std::min(table, (double)std::max<uint64_t>(opt.level_bytes, min_rows * 4ull * w));
+      resident += std::min(table, (double)std::max<uint64_t>(lb, min_rows * 4ull * w));
     } else {
       const double res_rows = std::min<double>((double)std::max<uint64_t>(opt.result_rows, 1), (double)opt.cap);
       resident += std::min(table, res_rows * 4.0 * w);
@@ -627,8 +638,9 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   if (opt.admit) {
     const uint64_t min_rows_a = (uint64_t)g.max_degree + 64;
     uint64_t cap_bytes = 0;
+    const uint64_t lb = level_buffer_bytes(ws, opt, qn);
     for (uint32_t w = 2; w < qn; ++w)
-      cap_bytes += std::max<uint64_t>(opt.level_bytes, min_rows_a * 4ull * w);
+      cap_bytes += std::max<uint64_t>(lb, min_rows_a * 4ull * w);
     const uint64_t res_rows =
         std::max<uint64_t>(std::min<uint64_t>(std::max<uint64_t>(opt.result_rows, opt.keep_on_device ? opt.cap : 0),
                                               opt.cap),
@@ -726,8 +738,9 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     L[1].cap_rows = L[1].nrows;
     R.stats.level_rows[1] = L[1].nrows;
     const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+    const uint64_t lb = level_buffer_bytes(ws, opt, qn);
     for (uint32_t w = 2; w < qn; ++w) {
-      uint64_t rows = std::max<uint64_t>(opt.level_bytes / (4ull * w), min_rows);
+      uint64_t rows = std::max<uint64_t>(lb / (4ull * w), min_rows);
       L[w].cap_rows = rows;
       L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
     }

@@ -201,7 +201,7 @@ __global__ void k_mlp_to_bf16(const float* __restrict__ w, __nv_bfloat16* __rest
 // ---------------------------------------------------------------------------
 struct PlanOut {
   int32_t order[kMaxPlanQ];
-  float work;     // predicted sum_k 2^{L_k}
+  float work;     // predicted sum of 2^{L_k} over the intermediate tables (widths 1 .. n-1)
   float peak;     // predicted max_k 2^{L_k} * 4 * (k + 1) bytes (the largest whole table)
   float pad[2];
   float logsize[kMaxPlanQ];  // L_k: predicted log2 rows of the table of width k + 1
@@ -260,7 +260,9 @@ __global__ void __launch_bounds__(288) k_plan(const PlanQuery* __restrict__ Qp, 
     L = L < 0.f ? 0.f : L;
     if (lane == 0) O.logsize[k] = L;
     const float rows = exp2f(L);
-    work += rows;
+    // the final table holds the embeddings, the same in every order (and,
+    // under a cap, the same number of rows): it does not rank orders
+    if (k + 1 < n) work += rows;
     peak = fmaxf(peak, rows * 4.f * (float)(k + 1));
   }
   if (lane == 0) {

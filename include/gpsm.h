@@ -155,7 +155,7 @@ typedef struct gpsm_match_info {
   uint64_t alg_bytes_join;   /* algorithmic bytes of the joins (roofline numerator) */
   double expand_ms;          /* summed device time of the join launches */
   double plan_ms;            /* learned-order planning */
-  double predicted_work;     /* learned order: predicted sum of table sizes */
+  double predicted_work;     /* learned order: predicted rows over the intermediate tables (final table excluded) */
   double predicted_peak;     /* learned order: predicted peak table bytes */
   int32_t order_fallback;    /* plain order used instead of the learned plan: 1 its predicted join memory is
                                 over the budget; 2 it is not predicted to scan under half the plain order's rows;
@@ -200,7 +200,8 @@ void gpsm_free(void* p);
  * edges q_edges[2*q_eoff[k]..]); rows are produced in device memory and
  * overwritten by the next query. orders: concatenated pos2id per query when
  * opts->order_mode is GPSM_ORDER_GIVEN. counts, capped, query_ms: nq each or
- * NULL. A throughput entry point with no counterpart in the reference, whose
+ * NULL (capped[k]: 1 the cap stopped query k, 2 opts->work_cap did). A
+ * throughput entry point with no counterpart in the reference, whose
  * run.cpp loops Match::match per query (main/run.cpp:60-97). */
 int gpsm_match_batch(gpsm_engine_t e, gpsm_graph_t g, uint32_t nq, const uint32_t* q_voff,
                      const uint32_t* q_labels, const uint64_t* q_eoff, const uint32_t* q_edges,
@@ -230,8 +231,7 @@ int gpsm_select_vertices_static(const uint32_t* d_labels, const uint32_t* d_offs
 /* The batch on `slots` engine slots of the graph's device (each its own
  * stream and workspace of slot_arena bytes, 0 = automatic), each slot
  * taking the next query when it finishes one, so queries overlap on the GPU.
- * Same outputs as gpsm_match_batch (capped[k] = 2 when opts->work_cap
- * stopped query k); device time is the span from the first slot's start to
+ * Same outputs as gpsm_match_batch; device time is the span from the first slot's start to
  * the last slot's end. */
 int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_voff,
                               const uint32_t* q_labels, const uint64_t* q_eoff,

@@ -679,14 +679,22 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     // back-neighbour descriptors for each added position p >= 1
     std::vector<BackNbr> hb;
     std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
+    // first estimate of candidates per row when extending to position p: the
+    // shortest average candidate-edge list among the placed neighbours (the
+    // driver is the shortest list of each row); later steps use what they saw
+    std::vector<double> ratio0(qn + 1, 4.0);
     for (uint32_t p = 1; p < qn; ++p) {
       back_off[p] = (uint32_t)hb.size();
       const uint32_t v = (uint32_t)pos2id[p];
+      double est = -1.0;
       for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
         const uint32_t w = Q.rcol[k];
         if ((uint32_t)R.id2pos[w] >= p) continue;
         const int e = Q.edge_between(w, v);
         const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
+        const double avg = (double)((d & 1) ? R.stats.size_rev[e] : R.stats.size_fwd[e]) /
+                           (double)std::max<uint32_t>(cnt[w], 1);
+        if (est < 0 || avg < est) est = avg;
         BackNbr b;
         b.col = (uint32_t)R.id2pos[w];
         b.pad = 0;
@@ -697,6 +705,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
         hb.push_back(b);
         back_cnt[p]++;
       }
+      if (est >= 0) ratio0[p] = std::max(est, 1.0 / 1024.0);
     }
     BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
     if (!hb.empty())
@@ -733,6 +742,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     const uint64_t cap = opt.cap;
     // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
     std::vector<Level> L(qn + 1);
+    for (uint32_t w = 1; w < qn; ++w) L[w].ratio = ratio0[w];
     L[1].buf = list[pos2id[0]];
     L[1].nrows = cnt[pos2id[0]];
     L[1].cap_rows = L[1].nrows;
@@ -835,6 +845,11 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
         budget = std::min<uint64_t>(out_cap, opt.step_cands);
       } else if (final_level) {
         uint64_t space = res_cap - res_used;
+        if (!opt.keep_on_device && res_used > 0 && cap - emitted > space &&
+            space < std::min<uint64_t>(res_cap, opt.step_cands) / 2) {
+          flush();  // a step into the little space left would be a small one
+          space = res_cap;
+        }
         out = res_buf + res_used * qn;
         if (cap - emitted <= space) {
           // the cap ends the query inside this buffer: rows past it are cut

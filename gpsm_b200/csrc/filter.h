@@ -68,6 +68,8 @@ struct StepState {
   unsigned long long blocks_done;  // persistent blocks finished
   unsigned long long cands;        // candidates of the admitted rows
   unsigned long long pad;
+  unsigned long long cand_end;     // end offset of the last admitted row's candidates
+  unsigned long long full;         // a row failed admission: later locate tiles skip their rows
 };
 
 // Per-row scratch of a join step: driver list (lo, hi32 of lo, length, j)

@@ -90,13 +90,25 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
                                                      unsigned long long* __restrict__ coff,
                                                      StepState* __restrict__ st, Lookback lb) {
   __shared__ LocateShared S;
-  if (threadIdx.x == 0) S.tile = lb_take_ticket(lb);
+  __shared__ uint32_t s_skip;
+  if (threadIdx.x == 0) {
+    S.tile = lb_take_ticket(lb);
+    // an earlier tile (smaller ticket, so earlier rows) already found a row
+    // past the budget: no row of this tile can be admitted
+    s_skip = *(volatile unsigned long long*)&st->full != 0;
+  }
   stage_back(S.back, back, nb);
   __syncthreads();
   const uint32_t tile = S.tile;
   const unsigned long long ntiles = (nrows + kLocBlock - 1) / kLocBlock;
   if ((unsigned long long)tile >= ntiles) {  // ticket base out of step with the device counter
     if (threadIdx.x == 0) atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
+    return;
+  }
+  if (s_skip) {
+    // publish a total past the budget so later tiles that are already
+    // working see every following row as not admitted
+    if (threadIdx.x < 32) lb_exclusive(lb, tile, budget + 1);
     return;
   }
   const unsigned long long i = (unsigned long long)tile * kLocBlock + threadIdx.x;
@@ -128,12 +140,20 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
   }
   __syncthreads();
   const unsigned long long off = S.prefix + mine;
+  // rows are admitted in order while all their candidates fit the budget;
+  // offsets grow with the row, so the admitted rows of a tile are a prefix
+  const bool fits = i < nrows && off + best_len <= budget;
+  const int nfit = __syncthreads_count(fits);
   if (i < nrows) {
     coff[i] = off;
-    // rows are admitted in order while all their candidates fit the budget
-    if (off + best_len <= budget) atomicMax(&st->rows, i + 1);
     if (i + 1 == nrows) coff[nrows] = off + best_len;
   }
+  if (nfit > 0 && threadIdx.x == (uint32_t)nfit - 1) {
+    atomicMax(&st->rows, i + 1);
+    atomicMax(&st->cand_end, off + best_len);
+  }
+  const unsigned long long in_tile = min((unsigned long long)kLocBlock, nrows - (unsigned long long)tile * kLocBlock);
+  if (threadIdx.x == 0 && (unsigned long long)nfit < in_tile) atomicExch(&st->full, 1ULL);
 }
 
 constexpr uint32_t kSpan = 1024;  // rows of one tile whose offsets are staged in shared memory
@@ -174,7 +194,8 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
   for (uint32_t i = threadIdx.x; i < ninj; i += blockDim.x) S.inj[i] = inj[i];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const unsigned long long nr = st->rows;     // rows admitted by k_locate
-  const unsigned long long ncand = nr ? coff[nr] : 0;
+  // coff[nr] may lie in a tile k_locate skipped; the admitted rows' end is exact
+  const unsigned long long ncand = nr ? st->cand_end : 0;
   const unsigned long long ntiles = (ncand + kExtTile - 1) / kExtTile;
   const uint32_t out_cols = cols + 1;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
@@ -196,7 +217,8 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
     const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
     const bool staged = span <= kSpan;
     if (staged)
-      for (uint32_t x = threadIdx.x; x <= span; x += blockDim.x) S.coff[x] = __ldg(coff + r0 + x);
+      for (uint32_t x = threadIdx.x; x <= span; x += blockDim.x)
+        S.coff[x] = r0 + x < nr ? __ldg(coff + r0 + x) : ncand;
     __syncthreads();
     uint32_t keep[kExtItems], yv[kExtItems];
     unsigned long long rv[kExtItems];

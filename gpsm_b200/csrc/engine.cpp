@@ -733,6 +733,8 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     js.drv = arena_alloc<uint4>(ws, js.rows);
     js.rng = arena_alloc<uint4>(ws, js.rng_entries);
     js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
+    js.tiles = (opt.step_cands + join_cands_per_extend_tile() - 1) / join_cands_per_extend_tile() + 2;
+    js.tile_row = arena_alloc<uint32_t>(ws, js.tiles);
     GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
     R.stats.level_rows.assign(qn + 1, 0);

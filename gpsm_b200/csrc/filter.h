@@ -78,9 +78,12 @@ struct JoinScratch {
   uint4* drv = nullptr;
   uint4* rng = nullptr;               // rows x nb list ranges (lo, lo>>32, length, 0)
   unsigned long long* coff = nullptr;
+  uint32_t* tile_row = nullptr;       // per extend tile: the row holding its first candidate
   uint64_t rows = 0;
   uint64_t rng_entries = 0;
+  uint64_t tiles = 0;                 // entries of tile_row
 };
+uint64_t join_cands_per_extend_tile();
 
 // One join step over input rows [row_begin, row_end) (in_cols columns,
 // row-major): rows are admitted in order while their candidates fit

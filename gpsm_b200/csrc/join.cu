@@ -41,8 +41,10 @@ constexpr int kLocBlock = 256;  // rows per locate tile
 constexpr int kExtBlock = 256;
 constexpr int kExtItems = 4;
 constexpr int kExtTile = kExtBlock * kExtItems;  // candidates per extend tile
-static uint32_t ext_grid() {  // persistent extend blocks
-  return (uint32_t)sm_count() * std::max<uint32_t>(1, std::min<uint32_t>(tuning().ext_blocks_per_sm, 8));
+static uint32_t ext_resident_per_sm();
+static uint32_t ext_grid() {  // persistent extend blocks: all resident at once
+  const uint32_t per_sm = std::min<uint32_t>(std::max<uint32_t>(1, tuning().ext_blocks_per_sm), ext_resident_per_sm());
+  return (uint32_t)sm_count() * per_sm;
 }
 
 __device__ __forceinline__ bool sorted_contains(const uint32_t* __restrict__ a, unsigned long long lo,
@@ -88,6 +90,7 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
                                                      unsigned long long nbrs_total, unsigned long long budget,
                                                      uint4* __restrict__ drv, uint4* __restrict__ rng,
                                                      unsigned long long* __restrict__ coff,
+                                                     uint32_t* __restrict__ tile_row, unsigned long long tile_cap,
                                                      StepState* __restrict__ st, Lookback lb) {
   __shared__ LocateShared S;
   __shared__ uint32_t s_skip;
@@ -147,6 +150,11 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
   if (i < nrows) {
     coff[i] = off;
     if (i + 1 == nrows) coff[nrows] = off + best_len;
+    // extend tiles whose first candidate lies in this row start at this row
+    if (best_len > 0)
+      for (unsigned long long T = (off + kExtTile - 1) / kExtTile;
+           T * kExtTile < off + best_len && T < tile_cap; ++T)
+        tile_row[T] = (uint32_t)i;
   }
   if (nfit > 0 && threadIdx.x == (uint32_t)nfit - 1) {
     atomicMax(&st->rows, i + 1);
@@ -163,8 +171,11 @@ struct ExtendShared {
   uint32_t inj[kMaxBack];  // columns whose query vertex has the new vertex's label
   uint32_t tile;
   unsigned long long prefix;
-  unsigned long long r0, r1;  // rows holding the tile's first and last candidate
+  unsigned long long r0, r1;  // rows holding the tile's first and (at most) last candidate
   uint32_t warp_cnt[kExtItems][kExtBlock / 32];
+  // kept candidates of each warp's slice, in lane order: row and new value
+  uint32_t kept_row[kExtItems][kExtBlock / 32][32];
+  uint32_t kept_val[kExtItems][kExtBlock / 32][32];
   unsigned long long coff[kSpan + 1];
 };
 
@@ -185,6 +196,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
                                                      uint32_t nb, unsigned long long nbrs_total,
                                                      const uint4* __restrict__ drv, const uint4* __restrict__ rng,
                                                      const unsigned long long* __restrict__ coff,
+                                                     const uint32_t* __restrict__ tile_row,
                                                      uint32_t* __restrict__ out, unsigned long long out_cap,
                                                      StepState* __restrict__ st, Lookback lb,
                                                      unsigned long long reserved, const uint32_t* __restrict__ inj,
@@ -198,6 +210,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
   const unsigned long long ncand = nr ? st->cand_end : 0;
   const unsigned long long ntiles = (ncand + kExtTile - 1) / kExtTile;
   const uint32_t out_cols = cols + 1;
+  const float inv_out_cols = 1.0f / (float)out_cols;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
   for (;;) {
     __syncthreads();
@@ -210,8 +223,11 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
     const unsigned long long t_first = (unsigned long long)tile * kExtTile;
     const unsigned long long t_last = min(t_first + kExtTile, ncand) - 1;
     if (threadIdx.x == 0) {
-      S.r0 = row_of(coff, nr, t_first);
-      S.r1 = row_of(coff, nr, t_last);
+      // k_locate recorded the row of every tile's first candidate; the row
+      // of the next tile's first candidate bounds this tile's last row
+      S.r0 = __ldg(tile_row + tile);
+      S.r1 = (unsigned long long)tile + 1 < ntiles ? min((unsigned long long)__ldg(tile_row + tile + 1), nr - 1)
+                                                    : nr - 1;
     }
     __syncthreads();
     const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
@@ -269,6 +285,11 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
     for (int k = 0; k < kExtItems; ++k) {
       bal[k] = __ballot_sync(0xffffffffu, keep[k]);
       if (lane == 0) S.warp_cnt[k][wid] = __popc(bal[k]);
+      if (keep[k]) {
+        const uint32_t q = __popc(bal[k] & ((1u << lane) - 1u));
+        S.kept_row[k][wid][q] = (uint32_t)rv[k];
+        S.kept_val[k][wid][q] = yv[k];
+      }
     }
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -304,13 +325,18 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
       const uint32_t words = n * out_cols;
       for (uint32_t base = 0; base < words; base += 32) {
         const uint32_t w = base + lane;
-        const uint32_t q = (w < words ? w : words - 1) / out_cols;  // q-th kept candidate of the slice
+        if (w >= words) break;
+        // q-th kept candidate of the slice, column c: w < 32 * 129, so the
+        // float quotient is within one of the exact one; fix it up
+        uint32_t q = __float2uint_rz(((float)w + 0.5f) * inv_out_cols);
+        if (q * out_cols > w) --q;
+        else if ((q + 1) * out_cols <= w) ++q;
         const uint32_t c = w - q * out_cols;
-        const uint32_t src = __fns(bal[k], 0, q + 1);  // lane holding it
-        const unsigned long long r = __shfl_sync(0xffffffffu, rv[k], src);
-        const uint32_t y = __shfl_sync(0xffffffffu, yv[k], src);
-        if (w < words && p0 + q < out_cap)
-          out[(p0 + q) * out_cols + c] = (c < cols) ? __ldg(in + (row_begin + r) * cols + c) : y;
+        if (p0 + q < out_cap) {
+          const uint32_t r = S.kept_row[k][wid][q];
+          out[(p0 + q) * out_cols + c] =
+              (c < cols) ? __ldg(in + (row_begin + r) * cols + c) : S.kept_val[k][wid][q];
+        }
       }
     }
   }
@@ -322,6 +348,17 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
     const unsigned long long done = atomicAdd(&st->blocks_done, 1ULL);
     if (done == gridDim.x - 1) atomicExch(lb.ticket, lb.base + reserved);
   }
+}
+
+// Blocks of k_extend one SM holds at once (registers and shared memory
+// decide it); asked once per process.
+static uint32_t ext_resident_per_sm() {
+  static const uint32_t n = [] {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, kExtBlock, 0) != cudaSuccess || b < 1) b = 1;
+    return (uint32_t)b;
+  }();
+  return n;
 }
 
 __global__ void k_gather_u64(const unsigned long long* __restrict__ src, const unsigned long long* __restrict__ idx,
@@ -354,20 +391,22 @@ static Lookback next_lb(Workspace& ws, uint64_t tiles) {
 }
 
 uint64_t join_rows_per_locate_tile() { return kLocBlock; }
+uint64_t join_cands_per_extend_tile() { return kExtTile; }
 
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
-  if (nrows > js.rows || nrows * nb > js.rng_entries) {
+  if (nrows > js.rows || nrows * nb > js.rng_entries || (budget + kExtTile - 1) / kExtTile > js.tiles) {
     set_last_error("join step: more rows than the step scratch holds");
     throw CudaError{cudaErrorInvalidValue, "join rows"};
   }
   const uint64_t ltiles = (nrows + kLocBlock - 1) / kLocBlock;
   Lookback lb1 = next_lb(ws, ltiles);
   k_locate<<<(uint32_t)ltiles, kLocBlock, 0, ws.stream>>>(in, in_cols, row_begin, nrows, d_back, nb, nbrs_total,
-                                                          budget, js.drv, js.rng, js.coff, d_st, lb1);
+                                                          budget, js.drv, js.rng, js.coff, js.tile_row, js.tiles,
+                                                          d_st, lb1);
   GPSM_LAUNCHED();
   // k_extend is persistent: blocks take tiles by ticket until the admitted
   // candidates run out, then each takes one terminating ticket. The host
@@ -377,8 +416,8 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + grid;
   Lookback lb2 = next_lb(ws, reserved);
   k_extend<<<grid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
-                                                  js.coff, out, out_cap, d_st, lb2, (unsigned long long)reserved, d_inj,
-                                                  ninj);
+                                                  js.coff, js.tile_row, out, out_cap, d_st, lb2,
+                                                  (unsigned long long)reserved, d_inj, ninj);
   GPSM_LAUNCHED();
 }
 

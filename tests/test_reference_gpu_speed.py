@@ -1,0 +1,68 @@
+"""The reference's own CUDA build against this engine on the small ER set
+(10,000 vertices, average degree 8, labels 1..8; 10 induced queries of 6
+vertices), through the same driver loop (main/run.cpp:70-97): per query,
+Match::match, IO::output (host verify + text), flush; `match used` is the
+loop's wall time. The 10 queries are repeated so that the millisecond timer
+resolves the loop. Both programs must write the same file; the engine must
+be faster. Prints both times and the ratio."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(ROOT, "tests", "golden")
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "GpSM.exe")
+OUR_EXE = os.path.join(ROOT, "gpsm_b200", "gpsm_run")
+REPEAT = 20
+
+
+def _repeat_queries(src, dst, times):
+    """Writes the queries of `src` `times` times, renumbered, with the
+    terminating `t # -1`."""
+    blocks, cur = [], None
+    for line in open(src):
+        if line.startswith("t #"):
+            if line.split()[2] == "-1":
+                break
+            cur = []
+            blocks.append(cur)
+        elif cur is not None:
+            cur.append(line)
+    with open(dst, "w") as f:
+        k = 0
+        for _ in range(times):
+            for b in blocks:
+                f.write(f"t # {k}\n")
+                f.writelines(b)
+                k += 1
+        f.write("t # -1\n")
+    return k
+
+
+def _match_ms(stderr):
+    m = re.search(r"match used:\s*(\d+)\s*ms", stderr)
+    assert m, stderr[-2000:]
+    return int(m.group(1))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_EXE), reason="reference build absent (oracle/ref.mk)")
+def test_engine_beats_reference_build_on_small_er(gpu, tmp_path):
+    data = os.path.join(G, "small_er_data.g")
+    query = tmp_path / "query.g"
+    nq = _repeat_queries(os.path.join(G, "small_er_query.g"), query, REPEAT)
+    runs = {}
+    for name, exe in (("reference", REF_EXE), ("engine", OUR_EXE)):
+        out = tmp_path / f"{name}.txt"
+        r = subprocess.run([exe, data, str(query), str(out), "0"], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs[name] = (_match_ms(r.stderr), open(out, "rb").read())
+    (t_ref, a_ref), (t_our, a_our) = runs["reference"], runs["engine"]
+    assert a_our == a_ref
+    ratio = t_ref / max(t_our, 1)
+    print(f"\nsmall ER, {nq} queries: reference build {t_ref} ms ({nq / max(t_ref, 1) * 1e3:.0f} q/s), "
+          f"engine {t_our} ms ({nq / max(t_our, 1) * 1e3:.0f} q/s), ratio {ratio:.2f}")
+    assert t_our < t_ref

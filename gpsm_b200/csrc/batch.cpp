@@ -16,6 +16,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -37,8 +38,12 @@ struct SlotPool {
 static std::mutex g_pool_mu;
 static std::vector<SlotPool*> g_pools;
 
+// Workspace bytes per slot: the caller's figure, else GPSM_ARENA_GB (the same
+// override the default engine reads), else half the free memory shared out,
+// at most 16 GiB each.
 uint64_t slot_arena_bytes(uint32_t slots, uint64_t per_slot) {
   if (per_slot) return per_slot;
+  if (const char* e = getenv("GPSM_ARENA_GB")) return (uint64_t)(atof(e) * (double)(1ull << 30));
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 2ull << 30;
   return std::min<uint64_t>(16ull << 30, (uint64_t)(free_b * 0.5 / std::max<uint32_t>(slots, 1)));

@@ -892,9 +892,13 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       if (trace_enabled()) {
         float ems = 0;
         cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
-        fprintf(stderr, "[gpsm] step level=%d rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu ms=%.3f\n",
-                lv, (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
-                (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ems);
+        const unsigned long long ab = admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull +
+                                      written * 4ull * (lv + 1);
+        fprintf(stderr,
+                "[gpsm] step level=%d nb=%u rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu "
+                "alg_bytes=%llu ms=%.3f\n",
+                lv, back_cnt[lv], (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
+                (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ab, ems);
       }
       if (admitted == 0) {
         if (final_level && !partial && res_used > 0) {  // make room and retry

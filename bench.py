@@ -255,10 +255,15 @@ def run_ours(args):
     result = None
     if rank == 0:
         cpu_rate, cores, done, secs = cpu_leg(wl, cap, args.cpu_seconds) if world == 1 else (None, 0, 0, 0)
+        # DRAM bytes per join step (k_locate + k_extend launch pair): the
+        # ratio of DRAM traffic to algorithmic bytes from one ncu capture of
+        # this workload, times this run's algorithmic bytes per step
         traffic = None
         tf = os.path.join(ROOT, "profiles", "expand_traffic.json")
-        if os.path.exists(tf):
-            traffic = json.load(open(tf)).get("bytes_per_launch")
+        if os.path.exists(tf) and expand_launches:
+            ratio = json.load(open(tf)).get("traffic_over_alg")
+            if ratio:
+                traffic = ratio * alg_bytes / (expand_launches / 2)
         result = {
             "metric": METRIC,
             "value": total_q / dev_s,
@@ -285,6 +290,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "kernel": "join step (k_locate + k_extend)", "peak_source": peak_kind,
+                         "traffic_per": "join step, scaled from profiles/expand_traffic.json",
+                         "alg_bytes_per_step": alg_bytes / (expand_launches / 2) if expand_launches else None,
                          "expand_launches": expand_launches, "expand_ms": expand_ms},
             "cpu_baseline": None if cpu_rate is None else {
                 "value": cpu_rate, "unit": "queries/s", "cores": cores, "kind": "port",

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "engine.h"
 #include "filter.h"
 #include "internal.h"
 
@@ -112,6 +113,24 @@ static int bits_of(uint64_t n) {
   return b;
 }
 
+// Stable LSD passes (8-bit digits at `shifts`) from a into b and back;
+// returns the buffer holding the sorted keys.
+static unsigned long long* radix_passes(Workspace& ws, unsigned long long* a, unsigned long long* b, uint64_t nk,
+                                        const std::vector<uint32_t>& shifts, uint32_t* hist,
+                                        unsigned long long* hoff) {
+  const uint32_t ntiles = (uint32_t)((nk + kSortTile - 1) / kSortTile);
+  for (uint32_t sh : shifts) {
+    if (nk == 0) break;
+    k_radix_hist<<<ntiles, kSortBlock, 0, ws.stream>>>(a, nk, sh, ntiles, hist);
+    GPSM_LAUNCHED();
+    launch_scan_u32(ws, hist, (uint64_t)256 * ntiles, hoff);
+    k_radix_scatter<<<ntiles, kSortBlock, 0, ws.stream>>>(a, b, nk, sh, ntiles, hoff);
+    GPSM_LAUNCHED();
+    std::swap(a, b);
+  }
+  return a;
+}
+
 // Builds offsets[n+1] and cols[2m] on the device from host edges (m pairs).
 // Scratch comes from ws.arena (reset first). Returns the device arrays,
 // allocated with cudaMalloc (the graph owns them).
@@ -152,17 +171,7 @@ void build_csr_device(Workspace& ws, uint32_t n, uint64_t m, const uint32_t* h_e
   std::vector<uint32_t> shifts;
   for (int sh = 0; sh < b; sh += 8) shifts.push_back(sh);
   for (int sh = 0; sh < b; sh += 8) shifts.push_back(32 + sh);
-  unsigned long long* src = ka;
-  unsigned long long* dst = kb;
-  for (uint32_t sh : shifts) {
-    if (nk == 0) break;
-    k_radix_hist<<<ntiles, kSortBlock, 0, s>>>(src, nk, sh, ntiles, hist);
-    GPSM_LAUNCHED();
-    launch_scan_u32(ws, hist, (uint64_t)256 * ntiles, hoff);
-    k_radix_scatter<<<ntiles, kSortBlock, 0, s>>>(src, dst, nk, sh, ntiles, hoff);
-    GPSM_LAUNCHED();
-    std::swap(src, dst);
-  }
+  unsigned long long* src = radix_passes(ws, ka, kb, nk, shifts, hist, hoff);
   launch_scan_u32(ws, deg, n + 1, off64);  // off64[i] = sum of deg[0..i)
   GPSM_CUDA(cudaMalloc(d_off, (uint64_t)(n + 1) * 4));
   GPSM_CUDA(cudaMalloc(d_cols, std::max<uint64_t>(nk, 1) * 4));
@@ -173,6 +182,133 @@ void build_csr_device(Workspace& ws, uint32_t n, uint64_t m, const uint32_t* h_e
     GPSM_LAUNCHED();
   }
   GPSM_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// Label runs: each adjacency list sorted by (neighbour label, id), and a
+// directory of its runs. Keys hold (vertex << lbits | label rank) in the
+// high word and the neighbour in the low word; the CSR already orders them
+// by (vertex, neighbour), so stable passes over the high word alone give
+// (vertex, label, neighbour) order.
+// ---------------------------------------------------------------------------
+__global__ void k_label_keys(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col,
+                             const uint32_t* __restrict__ lrank, uint32_t n, uint32_t lbits,
+                             unsigned long long* __restrict__ keys) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps)
+    for (uint32_t j = off[v] + lane; j < off[v + 1]; j += 32) {
+      const uint32_t u = col[j];
+      keys[j] = ((unsigned long long)((v << lbits) | lrank[u]) << 32) | u;
+    }
+}
+
+// Runs per vertex: positions where the high word changes (or the list starts).
+__global__ void k_label_runs_count(const uint32_t* __restrict__ off, const unsigned long long* __restrict__ keys,
+                                   uint32_t n, uint32_t* __restrict__ cnt) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    const uint32_t b = off[v], e = off[v + 1];
+    uint32_t c = 0;
+    for (uint32_t j = b + lane; j < e; j += 32) c += (j == b || (keys[j] >> 32) != (keys[j - 1] >> 32)) ? 1u : 0u;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) cnt[v] = c;
+  }
+}
+
+__global__ void k_label_runs_write(const uint32_t* __restrict__ off, const unsigned long long* __restrict__ keys,
+                                   uint32_t n, const unsigned long long* __restrict__ run_base,
+                                   const uint32_t* __restrict__ label_of_rank, uint32_t lmask,
+                                   uint32_t* __restrict__ lcol, uint2* __restrict__ runs) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    const uint32_t b = off[v], e = off[v + 1];
+    unsigned long long pos = run_base[v];
+    for (uint32_t j0 = b; j0 < e; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      bool start = false;
+      unsigned long long k = 0;
+      if (j < e) {
+        k = keys[j];
+        lcol[j] = (uint32_t)k;
+        start = j == b || (k >> 32) != (keys[j - 1] >> 32);
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, start);
+      if (start) runs[pos + __popc(bal & ((1u << lane) - 1u))] = make_uint2(label_of_rank[(k >> 32) & lmask], j);
+      pos += __popc(bal);
+    }
+  }
+}
+
+void build_label_runs(DeviceGraph& g, const uint32_t* h_lab) {
+  const uint32_t n = g.n;
+  const uint64_t nnz = g.nnz;
+  const uint32_t L = (uint32_t)g.h_labels.size();
+  const int vbits = bits_of(n), lbits = bits_of(std::max<uint32_t>(L, 2));
+  if (nnz == 0 || vbits + lbits > 32) return;  // the filter scans whole lists
+  std::vector<uint32_t> lrank(n);
+  for (uint32_t x = 0; x < n; ++x)
+    lrank[x] = (uint32_t)(std::lower_bound(g.h_labels.begin(), g.h_labels.end(), h_lab[x]) - g.h_labels.begin());
+  const uint32_t ntiles = (uint32_t)((nnz + kSortTile - 1) / kSortTile);
+  const uint64_t arena = 2 * nnz * 8 + (uint64_t)256 * ntiles * 4 + ((uint64_t)256 * ntiles + 1) * 8 +
+                         (uint64_t)(n + 1) * 16 + (uint64_t)L * 4 + (64ull << 20);
+  Workspace* ws = workspace_create(g.device, arena, 1u << 20);
+  try {
+    auto take = [&](size_t bytes) {
+      void* p = ws->arena.alloc(std::max<size_t>(bytes, 16));
+      if (!p) throw CudaError{cudaErrorMemoryAllocation, "label runs arena"};
+      return p;
+    };
+    unsigned long long* ka = (unsigned long long*)take(nnz * 8);
+    unsigned long long* kb = (unsigned long long*)take(nnz * 8);
+    uint32_t* hist = (uint32_t*)take((uint64_t)256 * ntiles * 4);
+    unsigned long long* hoff = (unsigned long long*)take(((uint64_t)256 * ntiles + 1) * 8);
+    uint32_t* d_lrank = (uint32_t*)take((uint64_t)n * 4);
+    uint32_t* d_cnt = (uint32_t*)take((uint64_t)(n + 1) * 4);
+    unsigned long long* d_base = (unsigned long long*)take((uint64_t)(n + 2) * 8);
+    uint32_t* d_labels = (uint32_t*)take((uint64_t)std::max<uint32_t>(L, 1) * 4);
+    cudaStream_t s = ws->stream;
+    GPSM_CUDA(cudaMemcpyAsync(d_lrank, lrank.data(), (uint64_t)n * 4, cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaMemcpyAsync(d_labels, g.h_labels.data(), (uint64_t)L * 4, cudaMemcpyHostToDevice, s));
+    const uint32_t vgrid = (uint32_t)std::min<uint64_t>(((uint64_t)n * 32 + 255) / 256, 148 * 64);
+    k_label_keys<<<vgrid, 256, 0, s>>>(g.off, g.col, d_lrank, n, (uint32_t)lbits, ka);
+    GPSM_LAUNCHED();
+    std::vector<uint32_t> shifts;
+    for (int sh = 0; sh < vbits + lbits; sh += 8) shifts.push_back(32 + sh);
+    unsigned long long* sorted = radix_passes(*ws, ka, kb, nnz, shifts, hist, hoff);
+    k_label_runs_count<<<vgrid, 256, 0, s>>>(g.off, sorted, n, d_cnt);
+    GPSM_LAUNCHED();
+    launch_scan_u32(*ws, d_cnt, n, d_base);  // d_base[n] = runs in all
+    unsigned long long total = 0;
+    GPSM_CUDA(cudaMemcpyAsync(&total, d_base + n, 8, cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    GPSM_CUDA(cudaMalloc(&g.lcol, nnz * 4));
+    GPSM_CUDA(cudaMalloc(&g.run_off, (uint64_t)(n + 1) * 4));
+    GPSM_CUDA(cudaMalloc(&g.runs, std::max<uint64_t>(total, 1) * sizeof(uint2)));
+    k_u64_to_u32<<<(n + 256) / 256, 256, 0, s>>>(d_base, n + 1, g.run_off);
+    GPSM_LAUNCHED();
+    k_label_runs_write<<<vgrid, 256, 0, s>>>(g.off, sorted, n, d_base, d_labels, (1u << lbits) - 1u, g.lcol,
+                                             g.runs);
+    GPSM_LAUNCHED();
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    uint32_t flags = 0;
+    GPSM_CUDA(cudaMemcpy(&flags, ws->d_flags, 4, cudaMemcpyDeviceToHost));
+    if (flags & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {
+      set_last_error("label runs: device wait limit or bounds check tripped");
+      throw CudaError{cudaErrorLaunchFailure, "label runs"};
+    }
+  } catch (...) {
+    cudaFree(g.lcol);
+    cudaFree(g.run_off);
+    cudaFree(g.runs);
+    g.lcol = g.run_off = nullptr;
+    g.runs = nullptr;
+    workspace_free(ws);
+    throw;
+  }
+  workspace_free(ws);
 }
 
 }  // namespace gpsm

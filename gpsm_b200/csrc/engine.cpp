@@ -467,13 +467,14 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       valid[i] = 1;
       simple.push_back(i);
     }
+  // refinement targets: (query vertex, its label) pairs
   std::vector<uint32_t> ref_off(simple.size()), ref_cnt(simple.size());
   for (size_t i = 0; i < simple.size(); ++i) {
     ref_off[i] = (uint32_t)params.size();
     for (uint32_t x : Q.in[simple[i]])
-      if (valid[x]) params.push_back(x), ref_cnt[i]++;
+      if (valid[x]) params.push_back(x), params.push_back(Q.lab[x]), ref_cnt[i]++;
     for (uint32_t x : Q.out[simple[i]])
-      if (valid[x]) params.push_back(x), ref_cnt[i]++;
+      if (valid[x]) params.push_back(x), params.push_back(Q.lab[x]), ref_cnt[i]++;
   }
   uint32_t* d_params = arena_alloc<uint32_t>(ws, params.size() + 1);
   if (!params.empty())
@@ -553,6 +554,8 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       d.ids = list[u];
       d.n = cnt[u];
       d.v = v;
+      d.lab = Q.lab[v];
+      d.pad = 0;
       d.item_base = items;
       items += cnt[u];
     }

@@ -107,6 +107,72 @@ __device__ __forceinline__ bool defer_heavy(uint32_t deg, uint32_t item, HeavyLi
   return true;
 }
 
+// Neighbours of a candidate that can matter for one target all carry the
+// target's label: above this degree the filter scans only that label's run
+// of the label-sorted list (same vertices, same ascending order) instead of
+// the whole list.
+constexpr uint32_t kRunMinDegree = 32;
+
+// [*rb, *re) of lcol: mu's neighbours with label l (empty when none). All
+// lanes of the warp call it and get the same range.
+__device__ __forceinline__ void label_run_warp(const GraphView& g, uint32_t mu, uint32_t l, uint32_t end,
+                                               uint32_t* rb, uint32_t* re) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t db = g.run_off[mu], de = g.run_off[mu + 1];
+  *rb = *re = 0;
+  for (uint32_t k0 = db; k0 < de; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    uint2 r = make_uint2(0u, 0u);
+    bool m = false;
+    if (k < de) {
+      r = g.runs[k];
+      m = r.x == l;
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, m);
+    if (bal) {
+      const uint32_t src = __ffs(bal) - 1;
+      const uint32_t kk = k0 + src;
+      *rb = __shfl_sync(0xffffffffu, r.y, src);
+      *re = kk + 1 < de ? g.runs[kk + 1].y : end;
+      return;
+    }
+  }
+}
+
+// The candidate's scan range for a target of label l: its label run when
+// the graph has runs and the list is long, else the whole id-sorted list.
+__device__ __forceinline__ const uint32_t* scan_range_warp(const GraphView& g, uint32_t mu, uint32_t l, uint32_t b,
+                                                           uint32_t e, uint32_t* rb, uint32_t* re) {
+  if (g.lcol && e - b > kRunMinDegree) {
+    label_run_warp(g, mu, l, e, rb, re);
+    return g.lcol;
+  }
+  *rb = b;
+  *re = e;
+  return g.col;
+}
+
+// Block version: warp 0 looks the run up; every thread of the block calls it.
+__device__ __forceinline__ const uint32_t* scan_range_block(const GraphView& g, uint32_t mu, uint32_t l, uint32_t b,
+                                                            uint32_t e, uint32_t* rb, uint32_t* re) {
+  __shared__ uint2 s_run;
+  if (!(g.lcol && e - b > kRunMinDegree)) {
+    *rb = b;
+    *re = e;
+    return g.col;
+  }
+  if (threadIdx.x < 32) {
+    uint32_t x, y;
+    label_run_warp(g, mu, l, e, &x, &y);
+    if (threadIdx.x == 0) s_run = make_uint2(x, y);
+  }
+  __syncthreads();
+  *rb = s_run.x;
+  *re = s_run.y;
+  __syncthreads();
+  return g.lcol;
+}
+
 __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __restrict__ list,
                                                  const uint32_t* __restrict__ count, uint32_t u,
                                                  const uint32_t* __restrict__ tgt, uint32_t ntgt,
@@ -128,8 +194,10 @@ __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __
       const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
       uint32_t* bmv = bm + (size_t)v * words;
       bool any = false;
-      for (uint32_t j = b + lane; j < e; j += 32) {
-        const uint32_t mv = g.col[j];
+      uint32_t rb, re;
+      const uint32_t* cl = scan_range_warp(g, mu, lv, b, e, &rb, &re);
+      for (uint32_t j = rb + lane; j < re; j += 32) {
+        const uint32_t mv = cl[j];
         const uint2 ld = g.labdeg[mv];
         if (ld.x == lv && ld.y >= dv) {
           atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
@@ -160,8 +228,10 @@ __global__ void __launch_bounds__(kHeavyBlock) k_explore_heavy(GraphView g, Heav
       const uint32_t v = tgt[3 * t], lv = tgt[3 * t + 1], dv = tgt[3 * t + 2];
       uint32_t* bmv = bm + (size_t)v * words;
       bool any = false;
-      for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-        const uint32_t mv = g.col[j];
+      uint32_t rb, re;
+      const uint32_t* cl = scan_range_block(g, mu, lv, b, e, &rb, &re);
+      for (uint32_t j = rb + threadIdx.x; j < re; j += blockDim.x) {
+        const uint32_t mv = cl[j];
         const uint2 ld = g.labdeg[mv];
         if (ld.x == lv && ld.y >= dv) {
           atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
@@ -183,8 +253,8 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
                                                 const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                 uint32_t* __restrict__ bm, uint32_t words,
                                                 const uint32_t* __restrict__ flags, HeavyList hl) {
-  extern __shared__ uint32_t s_tgt[];
-  for (uint32_t i = threadIdx.x; i < ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
+  extern __shared__ uint32_t s_tgt[];  // 2 * ntgt: x, label
+  for (uint32_t i = threadIdx.x; i < 2 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
   if (*flags & DF_EMPTY) return;
   const uint32_t lane = threadIdx.x & 31;
@@ -196,13 +266,15 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
     if (defer_heavy(e - b, mu, hl)) continue;
     for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t* bmv = bm + (size_t)s_tgt[t] * words;
+      const uint32_t* bmv = bm + (size_t)s_tgt[2 * t] * words;
       bool found = false;
-      for (uint32_t j0 = b; j0 < e; j0 += 32) {
+      uint32_t rb, re;
+      const uint32_t* cl = scan_range_warp(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
+      for (uint32_t j0 = rb; j0 < re; j0 += 32) {
         const uint32_t j = j0 + lane;
         bool hit = false;
-        if (j < e) {
-          const uint32_t mv = g.col[j];
+        if (j < re) {
+          const uint32_t mv = cl[j];
           hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
         }
         if (__any_sync(0xffffffffu, hit)) {
@@ -229,13 +301,15 @@ __global__ void __launch_bounds__(kHeavyBlock) k_refine_heavy(GraphView g, Heavy
     const uint32_t mu = hl.items[i];
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
     for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t* bmv = bm + (size_t)tgt[t] * words;
+      const uint32_t* bmv = bm + (size_t)tgt[2 * t] * words;
       bool found = false;
-      for (uint32_t j0 = b; j0 < e && !found; j0 += blockDim.x) {
+      uint32_t rb, re;
+      const uint32_t* cl = scan_range_block(g, mu, tgt[2 * t + 1], b, e, &rb, &re);
+      for (uint32_t j0 = rb; j0 < re && !found; j0 += blockDim.x) {
         const uint32_t j = j0 + threadIdx.x;
         bool hit = false;
-        if (j < e) {
-          const uint32_t mv = g.col[j];
+        if (j < re) {
+          const uint32_t mv = cl[j];
           hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
         }
         found = __syncthreads_or(hit);
@@ -275,9 +349,11 @@ __global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
     if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_warp(g, mu, cd.lab, b, e, &rb, &re);
     uint32_t c = 0;
-    for (uint32_t j = b + lane; j < e; j += 32) {
-      const uint32_t mv = g.col[j];
+    for (uint32_t j = rb + lane; j < re; j += 32) {
+      const uint32_t mv = cl[j];
       c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -301,13 +377,15 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
     if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_warp(g, mu, cd.lab, b, e, &rb, &re);
     unsigned long long pos = goff[w];
-    for (uint32_t j0 = b; j0 < e; j0 += 32) {
+    for (uint32_t j0 = rb; j0 < re; j0 += 32) {
       const uint32_t j = j0 + lane;
       uint32_t mv = 0;
       bool hit = false;
-      if (j < e) {
-        mv = g.col[j];
+      if (j < re) {
+        mv = cl[j];
         hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, hit);
@@ -332,9 +410,11 @@ __global__ void __launch_bounds__(kHeavyBlock) k_cedge_count_heavy(GraphView g, 
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_block(g, mu, cd.lab, b, e, &rb, &re);
     uint32_t c = 0;
-    for (uint32_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-      const uint32_t mv = g.col[j];
+    for (uint32_t j = rb + threadIdx.x; j < re; j += blockDim.x) {
+      const uint32_t mv = cl[j];
       c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
     }
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -369,13 +449,15 @@ __global__ void __launch_bounds__(kHeavyBlock) k_cedge_write_heavy(GraphView g, 
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_block(g, mu, cd.lab, b, e, &rb, &re);
     unsigned long long pos = goff[w];
-    for (uint32_t j0 = b; j0 < e; j0 += blockDim.x) {
+    for (uint32_t j0 = rb; j0 < re; j0 += blockDim.x) {
       const uint32_t j = j0 + threadIdx.x;
       uint32_t mv = 0;
       bool hit = false;
-      if (j < e) {
-        mv = g.col[j];
+      if (j < re) {
+        mv = cl[j];
         hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, hit);
@@ -515,7 +597,7 @@ void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, co
   if (ntgt == 0 || max_count == 0) return;
   HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(max_count, 148 * 16);
-  k_refine<<<blocks, 256, ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
+  k_refine<<<blocks, 256, 2 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
                                                                ws.d_flags, hl);
   GPSM_LAUNCHED();
   if (hl.items) {

@@ -9,10 +9,19 @@ struct GraphView {
   const uint32_t* __restrict__ off;
   const uint32_t* __restrict__ col;
   const uint2* __restrict__ labdeg;
+  const uint32_t* __restrict__ lcol;     // label-sorted lists (null: scan col)
+  const uint32_t* __restrict__ run_off;
+  const uint2* __restrict__ runs;
   uint32_t n;
 };
 
-inline GraphView view(const DeviceGraph& g) { return GraphView{g.off, g.col, g.labdeg, g.n}; }
+inline GraphView view(const DeviceGraph& g) {
+  return GraphView{g.off, g.col, g.labdeg, g.lcol, g.run_off, g.runs, g.n};
+}
+
+// Builds g.lcol / g.run_off / g.runs on the device (leaves them null when
+// vertex ids and label ranks do not fit one 32-bit key).
+void build_label_runs(DeviceGraph& g, const uint32_t* h_lab);
 
 // Candidates deferred by a warp kernel to a block-per-candidate kernel.
 struct HeavyList {
@@ -27,6 +36,8 @@ struct CedgeDir {
   const uint32_t* ids;           // final sorted candidate list of u
   uint32_t n;                    // |C(u)|
   uint32_t v;                    // target query vertex (its bitmap is probed)
+  uint32_t lab;                  // its label
+  uint32_t pad;
   unsigned long long item_base;  // first work item (index into counts/offsets)
 };
 

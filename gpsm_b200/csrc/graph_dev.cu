@@ -11,7 +11,10 @@
 //                candidates of a query vertex (label l, degree >= d) are a
 //                prefix of label l's group, so initialisation touches only
 //                those vertices instead of scanning all N (check_kernel,
-//                match/Match.cu:431-446).
+//                match/Match.cu:431-446);
+//   lcol, runs = every adjacency list sorted by (neighbour label, id) with a
+//                directory of its label runs (csr_build.cu): the filter
+//                scans only the neighbours that carry a target's label.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -117,6 +120,7 @@ static DeviceGraph* graph_finish(int device, uint32_t n, const uint32_t* off, co
     k_labdeg<<<std::min<uint32_t>((n + 255) / 256, 148 * 8), 256>>>(g->off, g->lab, n, g->labdeg);
     GPSM_LAUNCHED();
     GPSM_CUDA(cudaDeviceSynchronize());
+    build_label_runs(*g, lab);
   } catch (...) {
     cudaFree(g->off);
     cudaFree(g->col);
@@ -219,6 +223,7 @@ DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, 
     k_labdeg<<<std::min<uint32_t>((n + 255) / 256, 148 * 8), 256>>>(g->off, g->lab, n, g->labdeg);
     GPSM_LAUNCHED();
     GPSM_CUDA(cudaDeviceSynchronize());
+    build_label_runs(*g, lab);
   } catch (...) {
     cudaFree(g->off);
     cudaFree(g->col);
@@ -285,6 +290,9 @@ void graph_free(DeviceGraph* g) {
   cudaFree(g->lab);
   cudaFree(g->labdeg);
   cudaFree(g->lab_vtx);
+  cudaFree(g->lcol);
+  cudaFree(g->run_off);
+  cudaFree(g->runs);
   delete g;
 }
 

@@ -65,6 +65,12 @@ struct DeviceGraph {
   uint32_t* dir_col = nullptr;
   uint32_t* dir_lab = nullptr;
   uint32_t max_degree = 0;
+  // label runs: every adjacency list again, sorted by (neighbour label, id),
+  // with a directory of (label, first index) per run; lets the filter scan
+  // only a candidate's neighbours that carry one query vertex's label
+  uint32_t* lcol = nullptr;     // [nnz] or null (not built)
+  uint32_t* run_off = nullptr;  // [n+1] directory offsets per vertex
+  uint2* runs = nullptr;        // [run_off[n]] (label, index into lcol), labels ascending per vertex
   // label frequency as the reference computes it (Graph::inverse_num)
   uint64_t label_count(uint32_t label) const;
   // [begin, end) of lab_vtx for vertices with `label` and degree >= d

@@ -345,8 +345,9 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   char* d_out = arena_alloc<char>(ws, plan_out_bytes() * 9);
   cudaStream_t s = ws.stream;
   GPSM_CUDA(cudaMemcpyAsync(d_q, PQ.get(), sizeof(PlanQuery), cudaMemcpyHostToDevice, s));
-  // only the rows of the n query vertices matter; copy the whole table for simplicity
-  GPSM_CUDA(cudaMemcpyAsync(d_e, PE.get(), sizeof(PlanEdges), cudaMemcpyHostToDevice, s));
+  // only the rows of the n query vertices are read
+  GPSM_CUDA(cudaMemcpyAsync(d_e->log_size, PE->log_size, sizeof(float) * kMaxPlanQ * Q.n, cudaMemcpyHostToDevice, s));
+  GPSM_CUDA(cudaMemcpyAsync(d_e->log_avg, PE->log_avg, sizeof(float) * kMaxPlanQ * Q.n, cudaMemcpyHostToDevice, s));
   GPSM_CUDA(cudaMemcpyAsync(d_st, starts.data(), starts.size() * 4, cudaMemcpyHostToDevice, s));
   GPSM_CUDA(cudaMemcpyAsync(d_fixed, plain.data(), Q.n * 4, cudaMemcpyHostToDevice, s));
   launch_plan(s, opt.model, d_q, d_e, d_st, (uint32_t)starts.size(), d_fixed, d_out);

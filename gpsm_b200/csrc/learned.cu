@@ -196,9 +196,9 @@ __global__ void k_mlp_to_bf16(const float* __restrict__ w, __nv_bfloat16* __rest
 }
 
 // ---------------------------------------------------------------------------
-// planner: one warp per start vertex runs the greedy order; lanes evaluate
-// the frontier vertices with the MLP in parallel.
+// planner: one warp per start vertex runs the greedy order.
 // ---------------------------------------------------------------------------
+constexpr int kPlanWarps = 9;  // up to 8 greedy starts + the scored plain order
 struct PlanOut {
   int32_t order[kMaxPlanQ];
   float work;     // predicted sum of 2^{L_k} over the intermediate tables (widths 1 .. n-1)
@@ -207,15 +207,49 @@ struct PlanOut {
   float logsize[kMaxPlanQ];  // L_k: predicted log2 rows of the table of width k + 1
 };
 
+// Weights for the planner, laid out for lane-parallel evaluation: lane j of
+// a warp computes hidden units j and j + 32, so layer weights are stored
+// input-major (w1t[k][j] = W1[j][k]): a warp's 32 loads of one input row
+// hit 32 consecutive words.
+struct PlanSmem {
+  float w1t[kFeat][kHidden];
+  float b1[kHidden];
+  float w2t[kHidden][kHidden];
+  float b2[kHidden];
+  float w3[kHidden];
+  float b3;
+  float x[kPlanWarps][kFeat];    // features of the candidate a warp scores
+  float h1[kPlanWarps][kHidden];
+  float h2[kPlanWarps][kHidden];
+};
+
 // One warp per start vertex builds a greedy order; when `fixed` is given,
 // warp `nstarts` scores that order instead (same predictions, no choice).
-__global__ void __launch_bounds__(288) k_plan(const PlanQuery* __restrict__ Qp, const PlanEdges* __restrict__ E,
-                                              const uint32_t* __restrict__ starts, uint32_t nstarts,
-                                              const int32_t* __restrict__ fixed,
-                                              const __nv_bfloat16* __restrict__ wb, const float* __restrict__ wf,
-                                              PlanOut* __restrict__ outs) {
-  __shared__ MlpSmem S;
-  stage_weights(S, wb, wf);
+// A warp scores the frontier candidates one after another, its lanes
+// splitting the hidden units; each unit's sum runs over its inputs in the
+// same order as mlp_eval, and lane 0 forms the output sum in order, so the
+// predictions equal mlp_eval's.
+__global__ void __launch_bounds__(32 * kPlanWarps) k_plan(const PlanQuery* __restrict__ Qp,
+                                                          const PlanEdges* __restrict__ E,
+                                                          const uint32_t* __restrict__ starts, uint32_t nstarts,
+                                                          const int32_t* __restrict__ fixed,
+                                                          const __nv_bfloat16* __restrict__ wb,
+                                                          const float* __restrict__ wf, PlanOut* __restrict__ outs) {
+  __shared__ PlanSmem S;
+  for (int i = threadIdx.x; i < kHidden * kFeat; i += blockDim.x) {
+    const int j = i / kFeat, k = i % kFeat;
+    S.w1t[k][j] = __bfloat162float(wb[kW1 + i]);
+  }
+  for (int i = threadIdx.x; i < kHidden * kHidden; i += blockDim.x) {
+    const int j = i / kHidden, k = i % kHidden;
+    S.w2t[k][j] = __bfloat162float(wb[kW2 + i]);
+  }
+  for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+    S.b1[i] = wf[kB1 + i];
+    S.b2[i] = wf[kB2 + i];
+    S.w3[i] = __bfloat162float(wb[kW3 + i]);
+  }
+  if (threadIdx.x == 0) S.b3 = wf[kB3];
   __syncthreads();
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const bool follow = fixed && wid == nstarts;
@@ -230,27 +264,49 @@ __global__ void __launch_bounds__(288) k_plan(const PlanQuery* __restrict__ Qp, 
   float L = Q.log_cand[v0];
   if (lane == 0) O.logsize[0] = L;
   float work = exp2f(L), peak = exp2f(L) * 4.f;
+  float* x = S.x[wid];
+  float* h1 = S.h1[wid];
+  float* h2 = S.h2[wid];
   for (uint32_t k = 1; k < n; ++k) {
     float best = 1e30f;
     uint32_t bv = 0xffffffffu;
-    for (uint32_t v = lane; v < n; v += 32) {
+    for (uint32_t v = 0; v < n; ++v) {  // warp-uniform
       if (pq_has(P, v)) continue;
       if (!((Q.adj[v][0] & P[0]) | (Q.adj[v][1] & P[1]))) continue;
       if (follow && v != (uint32_t)fixed[k]) continue;
-      float x[kFeat], h1[kHidden], h2[kHidden];
-      step_features(Q, *E, P, k, v, x);
-      const float d = mlp_eval(S, x, h1, h2);
+      if (lane == 0) step_features(Q, *E, P, k, v, x);
+      __syncwarp();
+      float a0 = S.b1[lane], a1 = S.b1[lane + 32];
+#pragma unroll
+      for (int f = 0; f < kFeat; ++f) {
+        const float xf = x[f];
+        a0 = fmaf(S.w1t[f][lane], xf, a0);
+        a1 = fmaf(S.w1t[f][lane + 32], xf, a1);
+      }
+      h1[lane] = a0 > 0.f ? a0 : 0.f;
+      h1[lane + 32] = a1 > 0.f ? a1 : 0.f;
+      __syncwarp();
+      float c0 = S.b2[lane], c1 = S.b2[lane + 32];
+#pragma unroll 16
+      for (int f = 0; f < kHidden; ++f) {
+        const float hf = h1[f];
+        c0 = fmaf(S.w2t[f][lane], hf, c0);
+        c1 = fmaf(S.w2t[f][lane + 32], hf, c1);
+      }
+      h2[lane] = c0 > 0.f ? c0 : 0.f;
+      h2[lane + 32] = c1 > 0.f ? c1 : 0.f;
+      __syncwarp();
+      float d = 0.f;
+      if (lane == 0) {
+        float o = S.b3;
+        for (int f = 0; f < kHidden; ++f) o = fmaf(S.w3[f], h2[f], o);
+        d = o;
+      }
+      d = __shfl_sync(0xffffffffu, d, 0);
+      __syncwarp();  // x, h1, h2 are rewritten for the next candidate
       if (d < best || (d == best && v < bv)) {
         best = d;
         bv = v;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const uint32_t ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      if (ob < best || (ob == best && ov < bv)) {
-        best = ob;
-        bv = ov;
       }
     }
     if (bv == 0xffffffffu) break;  // disconnected (rejected earlier)
@@ -437,7 +493,7 @@ void model_predict(Model* M, const float* x, uint32_t n, float* y) {
 // is written after the nstarts greedy plans.
 void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const PlanEdges* d_e, const uint32_t* d_starts,
                  uint32_t nstarts, const int32_t* d_fixed, void* d_out) {
-  nstarts = std::min<uint32_t>(nstarts, 8);
+  nstarts = std::min<uint32_t>(nstarts, kPlanWarps - 1);
   const uint32_t warps = std::max<uint32_t>(1, nstarts + (d_fixed ? 1 : 0));
   k_plan<<<1, 32 * warps, 0, s>>>(d_q, d_e, d_starts, nstarts, d_fixed, M->wb, M->w, (PlanOut*)d_out);
   GPSM_LAUNCHED();

@@ -172,10 +172,11 @@ struct ExtendShared {
   uint32_t tile;
   unsigned long long prefix;
   unsigned long long r0, r1;  // rows holding the tile's first and (at most) last candidate
-  uint32_t warp_cnt[kExtItems][kExtBlock / 32];
-  // kept candidates of each warp's slice, in lane order: row and new value
-  uint32_t kept_row[kExtItems][kExtBlock / 32][32];
-  uint32_t kept_val[kExtItems][kExtBlock / 32][32];
+  uint32_t warp_sum[kExtBlock / 32];  // kept candidates per warp, then their exclusive prefix
+  uint32_t total;                     // kept candidates of the tile
+  // the tile's kept candidates in order: row (within the step) and new value
+  uint32_t kept_row[kExtTile];
+  uint32_t kept_val[kExtTile];
   unsigned long long coff[kSpan + 1];
 };
 
@@ -191,6 +192,24 @@ __device__ __forceinline__ unsigned long long row_of(const unsigned long long* _
   return lo;
 }
 
+// Injectivity: y differs from the row's columns that hold a query vertex
+// with the new vertex's label (a data vertex has one label, so y can only
+// repeat such a column).
+__device__ __forceinline__ bool injective(const ExtendShared& S, const uint32_t* __restrict__ row, uint32_t ninj,
+                                          uint32_t y) {
+  for (uint32_t c = 0; c < ninj; ++c)
+    if (__ldg(row + S.inj[c]) == y) return false;
+  return true;
+}
+
+// Persistent blocks take tiles of kExtTile consecutive candidates by
+// ticket. Thread i of a block takes candidates 4i .. 4i+3 of the tile: one
+// row search for the first, the next ones usually in the same row (its
+// driver range and row pointer are loaded once per row). Kept candidates
+// are counted per thread, scanned across the warp and block, placed after
+// the previous tiles by the decoupled look-back, staged in shared memory in
+// order, and the block writes the tile's output rows as one contiguous
+// span.
 __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict__ in, uint32_t cols,
                                                      unsigned long long row_begin, const BackNbr* __restrict__ back,
                                                      uint32_t nb, unsigned long long nbrs_total,
@@ -213,131 +232,151 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
   const float inv_out_cols = 1.0f / (float)out_cols;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
   for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) S.tile = lb_take_ticket(lb);
+    __syncthreads();  // the previous tile's shared state is no longer read
+    if (threadIdx.x == 0) {
+      const uint32_t tile = lb_take_ticket(lb);
+      S.tile = tile;
+      if ((unsigned long long)tile < ntiles) {
+        // k_locate recorded the row of every tile's first candidate; the row
+        // of the next tile's first candidate bounds this tile's last row
+        S.r0 = __ldg(tile_row + tile);
+        S.r1 = (unsigned long long)tile + 1 < ntiles ? min((unsigned long long)__ldg(tile_row + tile + 1), nr - 1)
+                                                      : nr - 1;
+      }
+    }
     __syncthreads();
     const uint32_t tile = S.tile;
     if ((unsigned long long)tile >= ntiles) break;
     const bool skip = *(volatile unsigned long long*)&st->done != 0;  // output cap reached
-    // rows spanned by this tile; their offsets go to shared memory when few
     const unsigned long long t_first = (unsigned long long)tile * kExtTile;
-    const unsigned long long t_last = min(t_first + kExtTile, ncand) - 1;
-    if (threadIdx.x == 0) {
-      // k_locate recorded the row of every tile's first candidate; the row
-      // of the next tile's first candidate bounds this tile's last row
-      S.r0 = __ldg(tile_row + tile);
-      S.r1 = (unsigned long long)tile + 1 < ntiles ? min((unsigned long long)__ldg(tile_row + tile + 1), nr - 1)
-                                                    : nr - 1;
-    }
-    __syncthreads();
+    const unsigned long long t_end = min(t_first + kExtTile, ncand);
     const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
     const bool staged = span <= kSpan;
     if (staged)
       for (uint32_t x = threadIdx.x; x <= span; x += blockDim.x)
         S.coff[x] = r0 + x < nr ? __ldg(coff + r0 + x) : ncand;
     __syncthreads();
-    uint32_t keep[kExtItems], yv[kExtItems];
-    unsigned long long rv[kExtItems];
-#pragma unroll
-    for (int k = 0; k < kExtItems; ++k) {
-      const unsigned long long t =
-          (unsigned long long)tile * kExtTile + (unsigned long long)k * kExtBlock + threadIdx.x;
-      keep[k] = 0;
-      yv[k] = 0;
-      rv[k] = 0;
-      if (skip || t >= ncand) continue;
-      unsigned long long r, kk;
+    uint32_t kr[kExtItems], ky[kExtItems];  // item k's row and value (valid where keep has bit k)
+    uint32_t keep = 0;
+    const unsigned long long tb = t_first + (unsigned long long)threadIdx.x * kExtItems;
+    if (!skip && tb < t_end) {
+      // row of candidate tb: the last row whose first candidate is <= tb
+      unsigned long long r, rstart, rend;
+      uint32_t li = 0;
       if (staged) {
-        uint32_t lo_ = 0, hi_ = (uint32_t)span;  // S.coff[lo_] <= t < S.coff[hi_]
+        uint32_t lo_ = 0, hi_ = (uint32_t)span;  // S.coff[lo_] <= tb < S.coff[hi_]
         while (hi_ - lo_ > 1) {
           const uint32_t mid = (lo_ + hi_) >> 1;
-          if (S.coff[mid] <= t) lo_ = mid;
+          if (S.coff[mid] <= tb) lo_ = mid;
           else hi_ = mid;
         }
-        r = r0 + lo_;
-        kk = t - S.coff[lo_];
+        li = lo_;
+        r = r0 + li;
+        rstart = S.coff[li];
+        rend = S.coff[li + 1];
       } else {
-        r = row_of(coff, nr, t);
-        kk = t - __ldg(coff + r);
+        r = row_of(coff, nr, tb);
+        rstart = __ldg(coff + r);
+        rend = r + 1 < nr ? __ldg(coff + r + 1) : ncand;
       }
-      const uint4 d = __ldg(drv + r);
-      const unsigned long long lo = ((unsigned long long)d.y << 32) | d.x;
+      uint4 d = __ldg(drv + r);
+      unsigned long long lo = ((unsigned long long)d.y << 32) | d.x;
       const uint32_t* __restrict__ nbrs = S.back[d.w].nbrs;
-      const uint32_t y = __ldg(nbrs + lo + kk);
-      rv[k] = r;
-      yv[k] = y;
-      bool ok = !(kk > 0 && __ldg(nbrs + lo + kk - 1) == y);  // parallel data edges: once
       const uint32_t* row = in + (row_begin + r) * cols;
-      // a data vertex has one label, so y can only repeat a column whose
-      // query vertex has the new vertex's label
-      for (uint32_t c = 0; ok && c < ninj; ++c) ok = __ldg(row + S.inj[c]) != y;
-      for (uint32_t j = 0; ok && j < nb; ++j) {
-        if (j == d.w) continue;
-        const uint4 g2 = __ldg(rng + r * nb + j);  // list of the row's j-th placed neighbour
-        const unsigned long long l2 = ((unsigned long long)g2.y << 32) | g2.x;
-        ok = sorted_contains(S.back[j].nbrs, l2, l2 + g2.z, y);
-      }
-      keep[k] = ok;
-    }
-    // in-order positions: slice k of the tile precedes slice k+1
-    uint32_t bal[kExtItems];
+
+      uint32_t prev = 0;
+      bool has_prev = tb > rstart;  // parallel data edges: each neighbour once
+      if (has_prev) prev = __ldg(nbrs + lo + (tb - rstart) - 1);
 #pragma unroll
-    for (int k = 0; k < kExtItems; ++k) {
-      bal[k] = __ballot_sync(0xffffffffu, keep[k]);
-      if (lane == 0) S.warp_cnt[k][wid] = __popc(bal[k]);
-      if (keep[k]) {
-        const uint32_t q = __popc(bal[k] & ((1u << lane) - 1u));
-        S.kept_row[k][wid][q] = (uint32_t)rv[k];
-        S.kept_val[k][wid][q] = yv[k];
+      for (int k = 0; k < kExtItems; ++k) {
+        const unsigned long long t = tb + k;
+        if (t >= t_end) break;
+        while (t >= rend) {  // the next row with candidates
+          ++r;
+          if (staged) {
+            ++li;
+            rstart = S.coff[li];
+            rend = S.coff[li + 1];
+          } else {
+            rstart = __ldg(coff + r);
+            rend = r + 1 < nr ? __ldg(coff + r + 1) : ncand;
+          }
+          d = __ldg(drv + r);
+          lo = ((unsigned long long)d.y << 32) | d.x;
+          nbrs = S.back[d.w].nbrs;
+          row = in + (row_begin + r) * cols;
+          has_prev = false;
+        }
+        const uint32_t y = __ldg(nbrs + lo + (t - rstart));
+        bool ok = !(has_prev && prev == y);
+        prev = y;
+        has_prev = true;
+        if (ok) ok = injective(S, row, ninj, y);
+        // y must lie in every other placed neighbour's list
+        for (uint32_t j = 0; ok && j < nb; ++j) {
+          if (j == d.w) continue;
+          const uint4 g2 = __ldg(rng + r * nb + j);
+          const unsigned long long l2 = ((unsigned long long)g2.y << 32) | g2.x;
+          ok = sorted_contains(S.back[j].nbrs, l2, l2 + g2.z, y);
+        }
+        kr[k] = (uint32_t)r;
+        ky[k] = y;
+        keep |= (ok ? 1u : 0u) << k;
+      }
+    }
+    // in-order positions: warp inclusive scan of the per-thread counts
+    const uint32_t cnt = __popc(keep);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += x;
+    }
+    if (lane == 31) S.warp_sum[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const uint32_t v = lane < kExtBlock / 32 ? S.warp_sum[lane] : 0;
+      uint32_t x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+      }
+      const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
+      if (lane < kExtBlock / 32) S.warp_sum[lane] = x - v;
+      const unsigned long long ex = lb_exclusive(lb, tile, tot);
+      if (lane == 0) {
+        S.prefix = ex;
+        S.total = tot;
+        if (ex + tot >= out_cap) atomicExch(&st->done, 1ULL);
+        if ((unsigned long long)tile == ntiles - 1) st->written = min(ex + tot, out_cap);
       }
     }
     __syncthreads();
-    if (threadIdx.x < 32) {
-      unsigned long long run = 0;
+    {
+      uint32_t pos = S.warp_sum[wid] + incl - cnt;
 #pragma unroll
-      for (int k = 0; k < kExtItems; ++k) {
-        const uint32_t v = lane < kExtBlock / 32 ? S.warp_cnt[k][lane] : 0;
-        uint32_t x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-          if (lane >= (uint32_t)o) x += y;
+      for (int k = 0; k < kExtItems; ++k)
+        if (keep & (1u << k)) {
+          S.kept_row[pos] = kr[k];
+          S.kept_val[pos] = ky[k];
+          ++pos;
         }
-        const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
-        if (lane < kExtBlock / 32) S.warp_cnt[k][lane] = (uint32_t)run + x - v;
-        run += tot;
-      }
-      const unsigned long long ex = lb_exclusive(lb, tile, run);
-      if (lane == 0) {
-        S.prefix = ex;
-        if (ex + run >= out_cap) atomicExch(&st->done, 1ULL);
-        if ((unsigned long long)tile == ntiles - 1) st->written = min(ex + run, out_cap);
-      }
     }
     __syncthreads();
     const unsigned long long prefix = S.prefix;
     if (prefix >= out_cap) continue;
-    // each warp's kept rows of slice k are one contiguous span of the output
-#pragma unroll
-    for (int k = 0; k < kExtItems; ++k) {
-      const uint32_t n = __popc(bal[k]);
-      if (n == 0) continue;
-      const unsigned long long p0 = prefix + S.warp_cnt[k][wid];
-      const uint32_t words = n * out_cols;
-      for (uint32_t base = 0; base < words; base += 32) {
-        const uint32_t w = base + lane;
-        if (w >= words) break;
-        // q-th kept candidate of the slice, column c: w < 32 * 129, so the
-        // float quotient is within one of the exact one; fix it up
-        uint32_t q = __float2uint_rz(((float)w + 0.5f) * inv_out_cols);
-        if (q * out_cols > w) --q;
-        else if ((q + 1) * out_cols <= w) ++q;
-        const uint32_t c = w - q * out_cols;
-        if (p0 + q < out_cap) {
-          const uint32_t r = S.kept_row[k][wid][q];
-          out[(p0 + q) * out_cols + c] =
-              (c < cols) ? __ldg(in + (row_begin + r) * cols + c) : S.kept_val[k][wid][q];
-        }
-      }
+    // the tile's rows are one contiguous span of the output
+    const uint32_t words = S.total * out_cols;
+    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+      // float quotient within one of the exact one (w < 2^18); fix it up
+      uint32_t q = __float2uint_rz(((float)w + 0.5f) * inv_out_cols);
+      if (q * out_cols > w) --q;
+      else if ((q + 1) * out_cols <= w) ++q;
+      const uint32_t c = w - q * out_cols;
+      if (prefix + q < out_cap)
+        out[(prefix + q) * out_cols + c] =
+            (c < cols) ? __ldg(in + (row_begin + S.kept_row[q]) * cols + c) : S.kept_val[q];
     }
   }
   // the last block to finish moves the ticket counter to the end of the

@@ -144,6 +144,29 @@ def test_edge_cases(gpu):
     assert _sorted_rows(out.embeddings()) == [(0, 1), (1, 0), (1, 2), (2, 1)]
 
 
+def test_dense_cliques_many_placed_neighbours(gpu):
+    """Clique queries on a dense graph: the last join steps probe up to six
+    placed neighbours (four by cursor, the rest by binary search) and
+    candidates have more than 32 neighbours (the filter scans label runs).
+    Every vertex order gives the backtracking oracle's embedding set."""
+    rng = np.random.default_rng(11)
+    n = 64
+    edges = [(a, b) for a in range(n) for b in range(a + 1, n) if rng.random() < 0.6]
+    g = _graph(n, edges, rng.integers(1, 3, n))
+    dg = gpu.DeviceGraph(g)
+    for k in (6, 7):
+        q = _query([1] * k, [(a, b) for a in range(k) for b in range(a + 1, k)])
+        rows, cnt = oracle.enumerate_embeddings(g, q)
+        ref = [tuple(x) for x in rows.tolist()]
+        assert cnt > 1000
+        out = gpu.match(dg, q)
+        assert out.count == cnt and _sorted_rows(out.embeddings()) == ref
+        for _ in range(3):
+            order = [int(x) for x in rng.permutation(k)]
+            out = gpu.match(dg, q, order=order)
+            assert out.count == cnt and _sorted_rows(out.embeddings()) == ref
+
+
 @pytest.mark.parametrize("seed", range(4))
 def test_random_graphs_against_backtracking(gpu, seed):
     g = W.rmat_graph(12, 24000, 12, 1.0, seed=seed)

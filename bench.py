@@ -206,7 +206,7 @@ def run_ours(args):
         run_step(args.slots)
     clocks = ClockSampler(local)
     step_ms, qms_all, launches, rows_total = [], [], 0, 0
-    alg_bytes, expand_ms, expand_launches = 0, 0.0, 0
+    alg_bytes, expand_ms, expand_launches, join_steps = 0, 0.0, 0, 0
     barrier(pg)
     clocks.start()
     t0 = time.perf_counter()
@@ -220,6 +220,7 @@ def run_ours(args):
         alg_bytes += info["alg_bytes_join"]
         expand_ms += info["expand_ms"]
         expand_launches += info["expand_launches"]
+        join_steps += info["join_steps"]
     wall = time.perf_counter() - t0
     barrier(pg)
     clk = clocks.stop()
@@ -255,15 +256,15 @@ def run_ours(args):
     result = None
     if rank == 0:
         cpu_rate, cores, done, secs = cpu_leg(wl, cap, args.cpu_seconds) if world == 1 else (None, 0, 0, 0)
-        # DRAM bytes per join step (k_locate + k_extend launch pair): the
+        # DRAM bytes per join step (its locate, check, scan and write launches): the
         # ratio of DRAM traffic to algorithmic bytes from one ncu capture of
         # this workload, times this run's algorithmic bytes per step
         traffic = None
         tf = os.path.join(ROOT, "profiles", "expand_traffic.json")
-        if os.path.exists(tf) and expand_launches:
+        if os.path.exists(tf) and join_steps:
             ratio = json.load(open(tf)).get("traffic_over_alg")
             if ratio:
-                traffic = ratio * alg_bytes / (expand_launches / 2)
+                traffic = ratio * alg_bytes / join_steps
         result = {
             "metric": METRIC,
             "value": total_q / dev_s,
@@ -289,9 +290,10 @@ def run_ours(args):
             "p99_ms": float(np.percentile(qms_all, 99)) if qms_all else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
-                         "kernel": "join step (k_locate + k_extend)", "peak_source": peak_kind,
+                         "kernel": "join step (k_locate + k_extend_check + k_scan_u32 + k_extend_write)", "peak_source": peak_kind,
                          "traffic_per": "join step, scaled from profiles/expand_traffic.json",
-                         "alg_bytes_per_step": alg_bytes / (expand_launches / 2) if expand_launches else None,
+                         "alg_bytes_per_step": alg_bytes / join_steps if join_steps else None,
+                         "join_steps": join_steps,
                          "expand_launches": expand_launches, "expand_ms": expand_ms},
             "cpu_baseline": None if cpu_rate is None else {
                 "value": cpu_rate, "unit": "queries/s", "cores": cores, "kind": "port",

@@ -121,7 +121,7 @@ class RequestInfo(C.Structure):
 
 class BatchInfo(C.Structure):
     _fields_ = [("device_ms", f64), ("expand_ms", f64), ("filter_ms", f64), ("rows", u64), ("launches", u64),
-                ("expand_launches", u64), ("alg_bytes_join", u64)]
+                ("expand_launches", u64), ("alg_bytes_join", u64), ("join_steps", u64)]
 
 
 def load(path=None):

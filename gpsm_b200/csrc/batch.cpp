@@ -72,7 +72,7 @@ struct BatchOut {
   std::vector<double> query_ms;
   std::vector<int> status;
   double device_ms = 0;
-  uint64_t launches = 0, expand_launches = 0, alg_bytes = 0;
+  uint64_t launches = 0, expand_launches = 0, alg_bytes = 0, join_steps = 0;
   double expand_ms = 0, filter_ms = 0;
   std::string first_msg;  // error text of the first failing query (set on a worker thread)
 };
@@ -139,6 +139,7 @@ int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const 
       std::lock_guard<std::mutex> lk(agg_mu);
       out.launches += R.stats.filter_launches + R.stats.expand_launches;
       out.expand_launches += R.stats.expand_launches;
+      out.join_steps += R.stats.join_steps;
       out.alg_bytes += R.stats.alg_bytes_join;
       out.expand_ms += R.stats.expand_ms;
       out.filter_ms += R.stats.filter_ms;
@@ -319,6 +320,7 @@ int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_vof
       for (uint32_t k = 0; k < nq; ++k) info->rows += out.rows[k];
       info->launches = out.launches;
       info->expand_launches = out.expand_launches;
+      info->join_steps = out.join_steps;
       info->alg_bytes_join = out.alg_bytes;
     }
     return rc;

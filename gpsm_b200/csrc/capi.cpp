@@ -507,6 +507,7 @@ int gpsm_match_batch(gpsm_engine_t eng, gpsm_graph_t g, uint32_t nq, const uint3
       bi.rows += R.rows;
       bi.launches += R.stats.filter_launches + R.stats.expand_launches;
       bi.expand_launches += R.stats.expand_launches;
+      bi.join_steps += R.stats.join_steps;
       bi.alg_bytes_join += R.stats.alg_bytes_join;
       bi.expand_ms += R.stats.expand_ms;
       bi.filter_ms += R.stats.filter_ms;

@@ -739,6 +739,9 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
     js.tiles = (opt.step_cands + join_cands_per_extend_tile() - 1) / join_cands_per_extend_tile() + 2;
     js.tile_row = arena_alloc<uint32_t>(ws, js.tiles);
+    js.kept = arena_alloc<uint2>(ws, js.tiles * join_cands_per_extend_tile());
+    js.tile_cnt = arena_alloc<uint32_t>(ws, js.tiles);
+    js.tile_off = arena_alloc<unsigned long long>(ws, js.tiles + 1);
     GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
     R.stats.level_rows.assign(qn + 1, 0);
@@ -884,7 +887,8 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
                        out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
       GPSM_CUDA(cudaEventRecord(ws.eve1, s));
-      exp_launches += 2;
+      exp_launches += 4;  // locate, check, scan, write
+      ++R.stats.join_steps;
       GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
       GPSM_CUDA(cudaStreamSynchronize(s));
       {

@@ -152,25 +152,11 @@ __device__ __forceinline__ const uint32_t* scan_range_warp(const GraphView& g, u
   return g.col;
 }
 
-// Block version: warp 0 looks the run up; every thread of the block calls it.
+// Block kernels: every warp looks the run up itself (the directory entries
+// come from L1 after the first warp), so no block barrier is needed.
 __device__ __forceinline__ const uint32_t* scan_range_block(const GraphView& g, uint32_t mu, uint32_t l, uint32_t b,
                                                             uint32_t e, uint32_t* rb, uint32_t* re) {
-  __shared__ uint2 s_run;
-  if (!(g.lcol && e - b > kRunMinDegree)) {
-    *rb = b;
-    *re = e;
-    return g.col;
-  }
-  if (threadIdx.x < 32) {
-    uint32_t x, y;
-    label_run_warp(g, mu, l, e, &x, &y);
-    if (threadIdx.x == 0) s_run = make_uint2(x, y);
-  }
-  __syncthreads();
-  *rb = s_run.x;
-  *re = s_run.y;
-  __syncthreads();
-  return g.lcol;
+  return scan_range_warp(g, mu, l, b, e, rb, re);
 }
 
 __global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __restrict__ list,

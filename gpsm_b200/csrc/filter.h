@@ -75,8 +75,8 @@ constexpr uint32_t kMaxBack = 128;  // query vertices are < 128 here; checked on
 struct StepState {
   unsigned long long rows;         // input rows admitted (a prefix of the step's rows)
   unsigned long long written;      // output rows written (<= out_cap)
-  unsigned long long done;         // set once the output reached out_cap
-  unsigned long long blocks_done;  // persistent blocks finished
+  unsigned long long next_tile;    // tile counter of the check pass
+  unsigned long long unused;
   unsigned long long cands;        // candidates of the admitted rows
   unsigned long long pad;
   unsigned long long cand_end;     // end offset of the last admitted row's candidates
@@ -90,6 +90,9 @@ struct JoinScratch {
   uint4* rng = nullptr;               // rows x nb list ranges (lo, lo>>32, length, 0)
   unsigned long long* coff = nullptr;
   uint32_t* tile_row = nullptr;       // per extend tile: the row holding its first candidate
+  uint2* kept = nullptr;              // tiles x 1024: kept (row, new value) of each tile, in order
+  uint32_t* tile_cnt = nullptr;       // kept candidates per tile
+  unsigned long long* tile_off = nullptr;  // tiles + 1: output row of each tile's first kept candidate
   uint64_t rows = 0;
   uint64_t rng_entries = 0;
   uint64_t tiles = 0;                 // entries of tile_row

@@ -10,21 +10,26 @@
 // list length, and none checks injectivity (io/IO.cpp:187-222 filters on the
 // host afterwards).
 //
-// Here a step is two kernels:
-//   k_locate  (one thread per input row) finds, for every placed neighbour
-//             w of v, the candidate-edge list N(row[w]) ∩ C(v) with an O(1)
-//             rank lookup in C(w)'s bitmap, keeps the shortest one as the
-//             row's driver, and turns the driver lengths into candidate
-//             offsets with a single-pass decoupled look-back scan. Rows are
-//             admitted in order while their candidates fit the step budget.
-//   k_extend  (one thread per candidate, persistent blocks) takes candidate
-//             t of row r from the driver list and keeps it if it differs
-//             from every value in the row (injectivity) and lies in every
-//             other placed neighbour's list (binary search: sorted-list
-//             intersection). Kept candidates are compacted in order with a
-//             warp ballot and a decoupled look-back over 1024-candidate
-//             tiles; each warp writes its output rows as one contiguous,
-//             coalesced span.
+// Here a step is four kernels:
+//   k_locate        (one thread per input row) finds, for every placed
+//                   neighbour w of v, the candidate-edge list N(row[w]) ∩ C(v)
+//                   with an O(1) rank lookup in C(w)'s bitmap, keeps the
+//                   shortest one as the row's driver, and turns the driver
+//                   lengths into candidate offsets with a single-pass
+//                   decoupled look-back scan. Rows are admitted in order while
+//                   their candidates fit the step budget.
+//   k_extend_check  (persistent blocks, tiles of 1024 candidates) takes
+//                   candidate t of row r from the driver list and keeps it if
+//                   it differs from every value in the row that could repeat
+//                   (injectivity) and lies in every other placed neighbour's
+//                   list (binary search: sorted-list intersection). Each tile
+//                   writes its kept (row, value) pairs in order and its count.
+//   k_scan_u32      turns the tile counts into output offsets.
+//   k_extend_write  copies each tile's kept rows (input row + new value) to
+//                   its offset: one contiguous, coalesced span per tile.
+// No block waits for another: an order-preserving look-back inside the
+// check kernel kept ~900 resident blocks waiting on their predecessors for
+// 40% of its time.
 // Work is spread by candidate, not by row, so a hub row with 60k candidates
 // and a row with one candidate cost the same per candidate. The output keeps
 // the reference's row order (input rows in order, each row's candidates
@@ -170,13 +175,9 @@ struct ExtendShared {
   BackNbr back[kMaxBack];
   uint32_t inj[kMaxBack];  // columns whose query vertex has the new vertex's label
   uint32_t tile;
-  unsigned long long prefix;
   unsigned long long r0, r1;  // rows holding the tile's first and (at most) last candidate
   uint32_t warp_sum[kExtBlock / 32];  // kept candidates per warp, then their exclusive prefix
   uint32_t total;                     // kept candidates of the tile
-  // the tile's kept candidates in order: row (within the step) and new value
-  uint32_t kept_row[kExtTile];
-  uint32_t kept_val[kExtTile];
   unsigned long long coff[kSpan + 1];
 };
 
@@ -202,24 +203,22 @@ __device__ __forceinline__ bool injective(const ExtendShared& S, const uint32_t*
   return true;
 }
 
-// Persistent blocks take tiles of kExtTile consecutive candidates by
-// ticket. Thread i of a block takes candidates 4i .. 4i+3 of the tile: one
+// Persistent blocks take tiles of kExtTile consecutive candidates from a
+// counter. Thread i of a block takes candidates 4i .. 4i+3 of the tile: one
 // row search for the first, the next ones usually in the same row (its
-// driver range and row pointer are loaded once per row). Kept candidates
-// are counted per thread, scanned across the warp and block, placed after
-// the previous tiles by the decoupled look-back, staged in shared memory in
-// order, and the block writes the tile's output rows as one contiguous
-// span.
-__global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict__ in, uint32_t cols,
-                                                     unsigned long long row_begin, const BackNbr* __restrict__ back,
-                                                     uint32_t nb, unsigned long long nbrs_total,
-                                                     const uint4* __restrict__ drv, const uint4* __restrict__ rng,
-                                                     const unsigned long long* __restrict__ coff,
-                                                     const uint32_t* __restrict__ tile_row,
-                                                     uint32_t* __restrict__ out, unsigned long long out_cap,
-                                                     StepState* __restrict__ st, Lookback lb,
-                                                     unsigned long long reserved, const uint32_t* __restrict__ inj,
-                                                     uint32_t ninj) {
+// driver range and row pointer are loaded once per row). The tile's kept
+// candidates go to kept[tile * kExtTile ...] in candidate order, their
+// number to tile_cnt[tile].
+__global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
+                                                           unsigned long long row_begin,
+                                                           const BackNbr* __restrict__ back, uint32_t nb,
+                                                           const uint4* __restrict__ drv,
+                                                           const uint4* __restrict__ rng,
+                                                           const unsigned long long* __restrict__ coff,
+                                                           const uint32_t* __restrict__ tile_row,
+                                                           uint2* __restrict__ kept, uint32_t* __restrict__ tile_cnt,
+                                                           StepState* __restrict__ st,
+                                                           const uint32_t* __restrict__ inj, uint32_t ninj) {
   __shared__ ExtendShared S;
   stage_back(S.back, back, nb);
   for (uint32_t i = threadIdx.x; i < ninj; i += blockDim.x) S.inj[i] = inj[i];
@@ -228,26 +227,22 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
   // coff[nr] may lie in a tile k_locate skipped; the admitted rows' end is exact
   const unsigned long long ncand = nr ? st->cand_end : 0;
   const unsigned long long ntiles = (ncand + kExtTile - 1) / kExtTile;
-  const uint32_t out_cols = cols + 1;
-  const float inv_out_cols = 1.0f / (float)out_cols;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
   for (;;) {
     __syncthreads();  // the previous tile's shared state is no longer read
     if (threadIdx.x == 0) {
-      const uint32_t tile = lb_take_ticket(lb);
-      S.tile = tile;
-      if ((unsigned long long)tile < ntiles) {
+      const unsigned long long tile = atomicAdd(&st->next_tile, 1ULL);
+      S.tile = (uint32_t)min(tile, ntiles);
+      if (tile < ntiles) {
         // k_locate recorded the row of every tile's first candidate; the row
         // of the next tile's first candidate bounds this tile's last row
         S.r0 = __ldg(tile_row + tile);
-        S.r1 = (unsigned long long)tile + 1 < ntiles ? min((unsigned long long)__ldg(tile_row + tile + 1), nr - 1)
-                                                      : nr - 1;
+        S.r1 = tile + 1 < ntiles ? min((unsigned long long)__ldg(tile_row + tile + 1), nr - 1) : nr - 1;
       }
     }
     __syncthreads();
     const uint32_t tile = S.tile;
     if ((unsigned long long)tile >= ntiles) break;
-    const bool skip = *(volatile unsigned long long*)&st->done != 0;  // output cap reached
     const unsigned long long t_first = (unsigned long long)tile * kExtTile;
     const unsigned long long t_end = min(t_first + kExtTile, ncand);
     const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
@@ -259,7 +254,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
     uint32_t kr[kExtItems], ky[kExtItems];  // item k's row and value (valid where keep has bit k)
     uint32_t keep = 0;
     const unsigned long long tb = t_first + (unsigned long long)threadIdx.x * kExtItems;
-    if (!skip && tb < t_end) {
+    if (tb < t_end) {
       // row of candidate tb: the last row whose first candidate is <= tb
       unsigned long long r, rstart, rend;
       uint32_t li = 0;
@@ -283,7 +278,6 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
       unsigned long long lo = ((unsigned long long)d.y << 32) | d.x;
       const uint32_t* __restrict__ nbrs = S.back[d.w].nbrs;
       const uint32_t* row = in + (row_begin + r) * cols;
-
       uint32_t prev = 0;
       bool has_prev = tb > rstart;  // parallel data edges: each neighbour once
       if (has_prev) prev = __ldg(nbrs + lo + (tb - rstart) - 1);
@@ -324,7 +318,8 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
         keep |= (ok ? 1u : 0u) << k;
       }
     }
-    // in-order positions: warp inclusive scan of the per-thread counts
+    // in-tile positions: warp inclusive scan of the per-thread counts, then
+    // the warps' exclusive prefix
     const uint32_t cnt = __popc(keep);
     uint32_t incl = cnt;
 #pragma unroll
@@ -342,50 +337,63 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= (uint32_t)o) x += y;
       }
-      const uint32_t tot = __shfl_sync(0xffffffffu, x, 31);
       if (lane < kExtBlock / 32) S.warp_sum[lane] = x - v;
-      const unsigned long long ex = lb_exclusive(lb, tile, tot);
-      if (lane == 0) {
-        S.prefix = ex;
-        S.total = tot;
-        if (ex + tot >= out_cap) atomicExch(&st->done, 1ULL);
-        if ((unsigned long long)tile == ntiles - 1) st->written = min(ex + tot, out_cap);
-      }
+      if (lane == 31) tile_cnt[tile] = x;
     }
     __syncthreads();
-    {
-      uint32_t pos = S.warp_sum[wid] + incl - cnt;
+    uint2* dst = kept + (unsigned long long)tile * kExtTile + S.warp_sum[wid] + incl - cnt;
 #pragma unroll
-      for (int k = 0; k < kExtItems; ++k)
-        if (keep & (1u << k)) {
-          S.kept_row[pos] = kr[k];
-          S.kept_val[pos] = ky[k];
-          ++pos;
+    for (int k = 0; k < kExtItems; ++k)
+      if (keep & (1u << k)) *dst++ = make_uint2(kr[k], ky[k]);
+  }
+}
+
+// Block per tile (grid-stride): the tile's kept rows go to output rows
+// tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
+// written.
+__global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
+                                                      unsigned long long row_begin, const uint2* __restrict__ kept,
+                                                      const uint32_t* __restrict__ tile_cnt,
+                                                      const unsigned long long* __restrict__ tile_off,
+                                                      uint32_t ntiles_max, uint32_t* __restrict__ out,
+                                                      unsigned long long out_cap, StepState* __restrict__ st) {
+  const uint32_t out_cols = cols + 1;
+  const float inv_out_cols = 1.0f / (float)out_cols;
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // rows of at most 32 words: lane -> (row within a group of rpw rows, column)
+  const uint32_t rpw = out_cols <= 32 ? 32 / out_cols : 0;
+  const uint32_t lane_q = rpw ? lane / out_cols : 0, lane_c = rpw ? lane - lane_q * out_cols : 0;
+  const bool lane_on = rpw && lane < rpw * out_cols;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->written = min(tile_off[ntiles_max], out_cap);
+  for (uint32_t tile = blockIdx.x; tile < ntiles_max; tile += gridDim.x) {
+    const uint32_t c = tile_cnt[tile];
+    const unsigned long long o = tile_off[tile];
+    if (c == 0 || o >= out_cap) continue;
+    const uint2* kt = kept + (unsigned long long)tile * kExtTile;
+    if (rpw) {
+      // each warp writes rpw whole rows per step: one contiguous span
+      for (uint32_t qb = wid * rpw; qb < c; qb += nwarps * rpw) {
+        const uint32_t q = qb + lane_q;
+        if (lane_on && q < c && o + q < out_cap) {
+          const uint2 e = __ldg(kt + q);
+          out[(o + q) * out_cols + lane_c] =
+              (lane_c < cols) ? __ldg(in + (row_begin + e.x) * cols + lane_c) : e.y;
         }
+      }
+      continue;
     }
-    __syncthreads();
-    const unsigned long long prefix = S.prefix;
-    if (prefix >= out_cap) continue;
-    // the tile's rows are one contiguous span of the output
-    const uint32_t words = S.total * out_cols;
+    const uint32_t words = c * out_cols;
     for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
       // float quotient within one of the exact one (w < 2^18); fix it up
       uint32_t q = __float2uint_rz(((float)w + 0.5f) * inv_out_cols);
       if (q * out_cols > w) --q;
       else if ((q + 1) * out_cols <= w) ++q;
-      const uint32_t c = w - q * out_cols;
-      if (prefix + q < out_cap)
-        out[(prefix + q) * out_cols + c] =
-            (c < cols) ? __ldg(in + (row_begin + S.kept_row[q]) * cols + c) : S.kept_val[q];
+      const uint32_t col = w - q * out_cols;
+      if (o + q < out_cap) {
+        const uint2 e = __ldg(kt + q);
+        out[(o + q) * out_cols + col] = (col < cols) ? __ldg(in + (row_begin + e.x) * cols + col) : e.y;
+      }
     }
-  }
-  // the last block to finish moves the ticket counter to the end of the
-  // range the host reserved, so the next launch's base is exact
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned long long done = atomicAdd(&st->blocks_done, 1ULL);
-    if (done == gridDim.x - 1) atomicExch(lb.ticket, lb.base + reserved);
   }
 }
 
@@ -394,7 +402,8 @@ __global__ void __launch_bounds__(kExtBlock) k_extend(const uint32_t* __restrict
 static uint32_t ext_resident_per_sm() {
   static const uint32_t n = [] {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend, kExtBlock, 0) != cudaSuccess || b < 1) b = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend_check, kExtBlock, 0) != cudaSuccess || b < 1)
+      b = 1;
     return (uint32_t)b;
   }();
   return n;
@@ -447,16 +456,17 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
                                                           budget, js.drv, js.rng, js.coff, js.tile_row, js.tiles,
                                                           d_st, lb1);
   GPSM_LAUNCHED();
-  // k_extend is persistent: blocks take tiles by ticket until the admitted
-  // candidates run out, then each takes one terminating ticket. The host
-  // reserves the worst case; the kernel's last block moves the counter to
-  // the end of the reservation.
-  const uint32_t grid = ext_grid();
-  const uint64_t reserved = (budget + kExtTile - 1) / kExtTile + grid;
-  Lookback lb2 = next_lb(ws, reserved);
-  k_extend<<<grid, kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, nbrs_total, js.drv, js.rng,
-                                                  js.coff, js.tile_row, out, out_cap, d_st, lb2,
-                                                  (unsigned long long)reserved, d_inj, ninj);
+  // check pass: persistent blocks take tiles from a counter until the
+  // admitted candidates run out
+  const uint64_t ntiles_max = (budget + kExtTile - 1) / kExtTile;
+  GPSM_CUDA(cudaMemsetAsync(js.tile_cnt, 0, std::max<uint64_t>(ntiles_max, 1) * sizeof(uint32_t), ws.stream));
+  k_extend_check<<<ext_grid(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff,
+                                                           js.tile_row, js.kept, js.tile_cnt, d_st, d_inj, ninj);
+  GPSM_LAUNCHED();
+  launch_scan_u32(ws, js.tile_cnt, std::max<uint64_t>(ntiles_max, 1), js.tile_off);
+  const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));
+  k_extend_write<<<wgrid, 256, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
+                                               (uint32_t)std::max<uint64_t>(ntiles_max, 1), out, out_cap, d_st);
   GPSM_LAUNCHED();
 }
 

@@ -176,6 +176,7 @@ typedef struct gpsm_batch_info {
   uint64_t launches;         /* kernels launched by the batch */
   uint64_t expand_launches;
   uint64_t alg_bytes_join;
+  uint64_t join_steps;       /* join steps (each: locate, check, scan, write launches) */
 } gpsm_batch_info;
 
 /* Matches one query. Replaces Match::match (match/Match.cu:1710-1966).

@@ -167,6 +167,19 @@ def test_dense_cliques_many_placed_neighbours(gpu):
             assert out.count == cnt and _sorted_rows(out.embeddings()) == ref
 
 
+def test_long_path_query_wide_rows(gpu):
+    """A 40-vertex path in a 100-vertex cycle: tables wider than 32 columns
+    (the write pass's general path); 200 embeddings (start, direction)."""
+    n, k = 100, 40
+    g = _graph(n, [(i, (i + 1) % n) for i in range(n)], [1] * n)
+    dg = gpu.DeviceGraph(g)
+    q = _query([1] * k, [(i, i + 1) for i in range(k - 1)])
+    rows, cnt = oracle.enumerate_embeddings(g, q)
+    assert cnt == 2 * n
+    out = gpu.match(dg, q)
+    assert out.count == cnt and _sorted_rows(out.embeddings()) == [tuple(x) for x in rows.tolist()]
+
+
 @pytest.mark.parametrize("seed", range(4))
 def test_random_graphs_against_backtracking(gpu, seed):
     g = W.rmat_graph(12, 24000, 12, 1.0, seed=seed)

@@ -289,8 +289,7 @@ int gpsm_engine_match(gpsm_engine_t eng, gpsm_graph_t g, uint32_t qn, const uint
     if (out_rows && mo.collect_rows) {
       // rows still on the device follow the flushed ones; the caller takes
       // the host block itself
-      if (R.d_rows && R.d_rows_count)
-        copy_to_host(*e->ws, R.host_rows.append(R.d_rows_count * qn), R.d_rows, R.d_rows_count * qn);
+      if (R.d_rows && R.d_rows_count) R.host_rows.append_from_device(*e->ws, R.d_rows, R.d_rows_count * qn);
       R.d_rows = nullptr;
       R.d_rows_count = 0;
       uint32_t* buf = R.host_rows.release();
@@ -326,7 +325,7 @@ int gpsm_match(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t q
   return rc;
 }
 
-void gpsm_free(void* p) { free(p); }
+void gpsm_free(void* p) { host_free(p); }
 
 int gpsm_last_levels(gpsm_engine_t eng, uint32_t n, uint64_t* level_in, uint64_t* level_cands, uint64_t* level_out) {
   gpsm_engine_s* e = engine_or_default(eng);

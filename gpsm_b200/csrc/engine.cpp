@@ -680,6 +680,10 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     R.host_rows.clear();
     R.d_rows = nullptr;
     R.d_rows_count = 0;
+    // a capped query that returns its rows gets a page-locked block for all
+    // of them up front: the device copies into it without a bounce buffer
+    if (opt.collect_rows && !opt.keep_on_device && opt.cap != ~0ULL)
+      R.host_rows.reserve_pinned(opt.cap * (uint64_t)qn);
     // back-neighbour descriptors for each added position p >= 1
     std::vector<BackNbr> hb;
     std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
@@ -800,7 +804,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
         res_used = 0;
         return;
       }
-      copy_to_host(ws, R.host_rows.append(res_used * qn), res_buf, res_used * qn);
+      R.host_rows.append_from_device(ws, res_buf, res_used * qn);
       res_used = 0;
     };
 
@@ -817,7 +821,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
         }
         if (opt.collect_rows) {
           R.host_rows.clear();
-          copy_to_host(ws, R.host_rows.append(n1), L[1].buf, n1);
+          R.host_rows.append_from_device(ws, L[1].buf, n1);
         }
       } else {
         res_used = n1;

@@ -108,41 +108,45 @@ struct MatchStats {
   uint64_t alg_bytes_filter = 0;
 };
 
-// Result rows on the host: one malloc'd block (a caller can take it with
-// release() and free() it), grown with realloc and never zero-filled; large
-// blocks ask for transparent huge pages, so first touch of a 10^7-row result
-// costs a fault per 2 MiB instead of per 4 KiB.
+// Result rows on the host: either a page-locked block from the library's
+// pool (reserve_pinned; the device copies into it directly) or a malloc'd
+// block grown with realloc and never zero-filled. A caller takes the block
+// with release() and gives it back with host_free (gpsm_free).
 class HostRows {
  public:
   HostRows() = default;
   HostRows(const HostRows&) = delete;
   HostRows& operator=(const HostRows&) = delete;
-  HostRows(HostRows&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_) { o.p_ = nullptr, o.n_ = o.cap_ = 0; }
-  HostRows& operator=(HostRows&& o) noexcept {
-    if (this != &o) {
-      free(p_);
-      p_ = o.p_, n_ = o.n_, cap_ = o.cap_;
-      o.p_ = nullptr, o.n_ = o.cap_ = 0;
-    }
-    return *this;
+  HostRows(HostRows&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_), pinned_(o.pinned_) {
+    o.p_ = nullptr, o.n_ = o.cap_ = 0, o.pinned_ = false;
   }
-  ~HostRows() { free(p_); }
+  HostRows& operator=(HostRows&& o) noexcept;
+  ~HostRows();
   uint64_t size() const { return n_; }  // words
   bool empty() const { return n_ == 0; }
   const uint32_t* data() const { return p_; }
   void clear() { n_ = 0; }
+  // take a pool block for `words` words if nothing is held yet (no-op when
+  // the pool is at its limit)
+  void reserve_pinned(uint64_t words);
   // room for `words` more words at the end; the size grows by that much
   uint32_t* append(uint64_t words);
+  // append `words` words copied from device memory on ws's stream
+  void append_from_device(Workspace& ws, const uint32_t* d_src, uint64_t words);
   uint32_t* release() {
     uint32_t* q = p_;
-    p_ = nullptr, n_ = cap_ = 0;
+    p_ = nullptr, n_ = cap_ = 0, pinned_ = false;
     return q;
   }
 
  private:
   uint32_t* p_ = nullptr;
   uint64_t n_ = 0, cap_ = 0;
+  bool pinned_ = false;
 };
+
+// Frees a result block: back to the pool if it came from there, else free().
+void host_free(void* p);
 
 struct MatchResult {
   uint64_t rows = 0;

@@ -1,34 +1,140 @@
 // Result rows on their way to the caller's host memory.
 //
-// A capped query of 10^7 rows and 12 columns returns 480 MB. Copying it
-// with one pageable cudaMemcpy into a freshly zero-filled std::vector spent
-// most of its time in 4 KiB page faults and in the driver's own bounce
-// copies. Here the rows go through two pinned staging buffers per workspace
-// (the DMA of one chunk overlaps the host copy of the previous one) into a
+// A capped query of 10^7 rows and 12 columns returns 480 MB; a serving loop
+// returns one such block per request. Two paths:
+//
+// Pooled (the usual one): a process-wide pool of page-locked blocks. A query
+// with an embedding cap takes a block large enough for cap rows before its
+// joins start; the device copies rows straight into it (one DMA per flush,
+// no bounce copy, no page faults: the block was touched and pinned when the
+// pool grew). The caller gets the block itself, and gpsm_free gives it back
+// to the pool, so the next request reuses it. The pool pins at most
+// GPSM_HOST_POOL_GB (default 8) GiB; past that, queries use the other path.
+//
+// Malloc'd: rows go through two pinned staging buffers per workspace (the
+// DMA of one chunk overlaps the host copy of the previous one) into a
 // malloc'd block that grows with realloc (mremap for large blocks: no copy)
-// and is advised for transparent huge pages. The block is handed to the
-// caller as is (gpsm_free releases it).
+// and is advised for transparent huge pages; gpsm_free frees it.
 #include <sys/mman.h>
 #include <unistd.h>
 
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <unordered_map>
 
 #include "engine.h"
 
 namespace gpsm {
 
+namespace {
+
+struct HostPool {
+  std::mutex mu;
+  std::multimap<uint64_t, void*> free_blocks;  // capacity bytes -> block
+  std::unordered_map<void*, uint64_t> owned;   // every pool block -> capacity bytes
+  uint64_t pinned = 0;
+  uint64_t limit = 0;
+  HostPool() {
+    const char* e = getenv("GPSM_HOST_POOL_GB");
+    limit = (uint64_t)((e ? atof(e) : 8.0) * (double)(1ull << 30));
+  }
+};
+
+HostPool& pool() {
+  static HostPool* p = new HostPool();  // lives until exit: blocks may be freed late
+  return *p;
+}
+
+// A pinned block of at least `bytes`, or null when the pool is at its limit
+// or pinning fails (the caller then uses malloc'd memory).
+void* pool_acquire(uint64_t bytes, uint64_t* cap) {
+  HostPool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.free_blocks.lower_bound(bytes);
+  if (it != P.free_blocks.end() && it->first <= 2 * bytes + (64ull << 20)) {
+    void* b = it->second;
+    *cap = it->first;
+    P.free_blocks.erase(it);
+    return b;
+  }
+  // size classes: multiples of 64 MiB
+  const uint64_t size = (bytes + (64ull << 20) - 1) & ~((64ull << 20) - 1);
+  if (P.pinned + size > P.limit) return nullptr;
+  void* b = nullptr;
+  if (posix_memalign(&b, 2ull << 20, size) != 0) return nullptr;
+  madvise(b, size, MADV_HUGEPAGE);
+  memset(b, 0, size);  // fault the pages in now, once
+  if (cudaHostRegister(b, size, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    free(b);
+    return nullptr;
+  }
+  P.pinned += size;
+  P.owned[b] = size;
+  *cap = size;
+  return b;
+}
+
+}  // namespace
+
+bool host_pool_release(void* p) {
+  if (!p) return false;
+  HostPool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.owned.find(p);
+  if (it == P.owned.end()) return false;
+  P.free_blocks.emplace(it->second, p);
+  return true;
+}
+
+void host_free(void* p) {
+  if (!host_pool_release(p)) free(p);
+}
+
+HostRows::~HostRows() { host_free(p_); }
+
+HostRows& HostRows::operator=(HostRows&& o) noexcept {
+  if (this != &o) {
+    host_free(p_);
+    p_ = o.p_, n_ = o.n_, cap_ = o.cap_, pinned_ = o.pinned_;
+    o.p_ = nullptr, o.n_ = o.cap_ = 0, o.pinned_ = false;
+  }
+  return *this;
+}
+
+void HostRows::reserve_pinned(uint64_t words) {
+  if (p_ || words == 0) return;
+  uint64_t cap = 0;
+  void* b = pool_acquire(words * sizeof(uint32_t), &cap);
+  if (!b) return;
+  p_ = static_cast<uint32_t*>(b);
+  cap_ = cap / sizeof(uint32_t);
+  n_ = 0;
+  pinned_ = true;
+}
+
 uint32_t* HostRows::append(uint64_t words) {
   if (n_ + words > cap_) {
     uint64_t want = std::max<uint64_t>(n_ + words, cap_ + cap_ / 2);
     want = std::max<uint64_t>(want, 1024);
-    void* q = realloc(p_, want * sizeof(uint32_t));
+    void* q = nullptr;
+    if (pinned_) {
+      // a pool block cannot grow in place: move to malloc'd memory
+      q = malloc(want * sizeof(uint32_t));
+      if (q && n_) memcpy(q, p_, n_ * sizeof(uint32_t));
+      if (q) host_pool_release(p_);
+    } else {
+      q = realloc(p_, want * sizeof(uint32_t));
+    }
     if (!q) {
       set_last_error("host allocation of result rows failed");
       throw CudaError{cudaErrorMemoryAllocation, "host rows"};
     }
     p_ = static_cast<uint32_t*>(q);
+    pinned_ = false;
     cap_ = want;
     const size_t bytes = want * sizeof(uint32_t);
     if (bytes >= (8u << 20)) {
@@ -42,6 +148,17 @@ uint32_t* HostRows::append(uint64_t words) {
   uint32_t* at = p_ + n_;
   n_ += words;
   return at;
+}
+
+void HostRows::append_from_device(Workspace& ws, const uint32_t* d_src, uint64_t words) {
+  if (words == 0) return;
+  uint32_t* dst = append(words);
+  if (pinned_) {
+    GPSM_CUDA(cudaMemcpyAsync(dst, d_src, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, ws.stream));
+    GPSM_CUDA(cudaStreamSynchronize(ws.stream));
+  } else {
+    copy_to_host(ws, dst, d_src, words);
+  }
 }
 
 void copy_to_host(Workspace& ws, uint32_t* dst, const uint32_t* d_src, uint64_t words) {

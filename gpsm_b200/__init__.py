@@ -378,11 +378,12 @@ class Server:
     joins when their predicted join memory fits memory_budget bytes."""
 
     def __init__(self, dgraph, slots=4, memory_budget=0, slot_arena=0, cap=None, order=None, model=None,
-                 collect_rows=False):
+                 collect_rows=False, work_cap=0):
         lib = _lib.load()
         self._lib = lib
         opts = _lib.MatchOpts()
         opts.cap = int(cap or 0)
+        opts.work_cap = int(work_cap)
         if order == "learned":
             opts.order_mode = _lib.GPSM_ORDER_LEARNED
             opts.model = model.handle
@@ -400,14 +401,22 @@ class Server:
                                                 C.byref(t)), "gpsm_server_submit")
         return t.value, query.n
 
-    def wait(self, ticket, timeout=-1.0):
+    def wait(self, ticket, timeout=-1.0, raise_on_error=True):
+        """The request's info (status, times, rows, ...); with
+        raise_on_error=False a failed request returns its info (status < 0,
+        "error" = the engine's text) instead of raising."""
         tid, qn = ticket
         info = _lib.RequestInfo()
+        info.status = 1  # stays 1 when the call fails before filling info (bad ticket, timeout)
         out = _lib.vp()
         idm = np.zeros(qn, np.int32)
         rc = self._lib.gpsm_server_wait(self.handle, tid, float(timeout), C.byref(info),
                                         C.byref(out) if self.collect else None, _lib.ptr(idm))
-        _lib.check(rc, "gpsm_server_wait")
+        if rc != 0 and (raise_on_error or info.status == 1):
+            _lib.check(rc, "gpsm_server_wait")
+        if rc != 0:
+            return {k: getattr(info, k) for k, _ in _lib.RequestInfo._fields_} | {
+                "error": self._lib.gpsm_last_error().decode(errors="replace")}
         d = {k: getattr(info, k) for k, _ in _lib.RequestInfo._fields_}
         if self.collect:
             # the table in join-column order (as the reference returns it);

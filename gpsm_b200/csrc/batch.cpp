@@ -173,6 +173,7 @@ struct Request {
   std::vector<uint32_t> lab, edges;
   double t_submit = 0, t_start = 0, t_admit = 0, t_end = 0;
   int status = 1;  // 1 = pending
+  std::string err;  // error text of a failed request (set on the slot's thread)
   uint64_t rows = 0;
   int capped = 0;
   double device_ms = 0;
@@ -261,8 +262,9 @@ struct Server {
       {
         std::lock_guard<std::mutex> lk(mu);
         r->status = rc;
+        if (rc != GPSM_OK) r->err = last_error();
         r->rows = R.rows;
-        r->capped = R.capped ? 1 : 0;
+        r->capped = R.capped ? 1 : (R.stats.aborted ? 2 : 0);
         r->device_ms = R.stats.device_ms;
         if (collect && rc == GPSM_OK) {
           r->result = std::move(R.host_rows);
@@ -408,6 +410,7 @@ int gpsm_server_wait(gpsm_server_t h, uint64_t ticket, double timeout_s, gpsm_re
   if (id_map)
     for (uint32_t i = 0; i < r->qn; ++i) id_map[i] = i < r->id2pos.size() ? r->id2pos[i] : -1;
   const int st = r->status;
+  if (st != GPSM_OK) set_last_error(r->err);  // the failing slot thread's text, on the caller's thread
   S->all.erase(it);
   delete r;
   return st;

@@ -504,15 +504,31 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) initialized[Q.rcol[k]] = 1;
   }
   // ---- refinement: 4 rounds + 1 emptiness check (match/Match.cu:848-890) ----
-  for (int k = 0; k < 5; ++k)
-    for (size_t i = 0; i < simple.size(); ++i) {
-      const uint32_t u = simple[i];
-      launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true);
-      ++launches;
-      if (k == 4 || ref_cnt[i] == 0) continue;
-      launch_refine(ws, g, list[u], counts + u, bound[u], u, d_params + ref_off[i], ref_cnt[i], bm);
-      ++launches;
-    }
+  // Launches that would change nothing exit at once (RefineStamp): the
+  // rounds and their order are the reference's, so the sets are the same.
+  {
+    uint32_t* stamp = arena_alloc<uint32_t>(ws, qn);
+    GPSM_CUDA(cudaMemsetAsync(stamp, 0, sizeof(uint32_t) * qn, s));
+    std::vector<uint32_t> last_refine(qn, 0), last_compact(qn, 0);
+    uint32_t seq = 0;
+    for (int k = 0; k < 5; ++k)
+      for (size_t i = 0; i < simple.size(); ++i) {
+        const uint32_t u = simple[i];
+        // the first refinement-phase compaction of u always runs: explore
+        // may have removed candidates after u's compaction in the init loop
+        launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true, stamp, u, last_compact[u]);
+        last_compact[u] = seq;
+        ++launches;
+        if (k == 4 || ref_cnt[i] == 0) continue;
+        RefineStamp rs;
+        rs.stamp = stamp;
+        rs.prev = last_refine[u];
+        rs.seq = ++seq;
+        launch_refine(ws, g, list[u], counts + u, bound[u], u, d_params + ref_off[i], ref_cnt[i], bm, rs);
+        last_refine[u] = seq;
+        ++launches;
+      }
+  }
   // ---- final candidate lists with ranks -----------------------------------
   for (uint32_t u = 0; u < qn; ++u) {
     launch_compact(ws, bm_of(u), W, list[u], rank + (size_t)u * W, counts + u, true);

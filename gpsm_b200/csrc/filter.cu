@@ -38,11 +38,15 @@ __global__ void __launch_bounds__(kCompactBlock) k_compact(const uint32_t* __res
                                                           uint32_t* __restrict__ list,
                                                           uint32_t* __restrict__ rank,
                                                           uint32_t* __restrict__ count, Lookback lb,
-                                                          uint32_t set_empty_flag) {
+                                                          uint32_t set_empty_flag, const uint32_t* __restrict__ stamp,
+                                                          uint32_t u, uint32_t prev) {
   __shared__ uint32_t s_tile;
   __shared__ unsigned long long s_prefix;
   if (threadIdx.x == 0) s_tile = lb_take_ticket(lb);
   __syncthreads();
+  // C(u) unchanged since the last compaction: list and count are current
+  // (every block has taken its ticket, so the host's ticket base stays exact)
+  if (stamp && prev && stamp[u] <= prev) return;
   const uint32_t tile = s_tile;
   const uint32_t ntiles_c = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
   if (tile >= ntiles_c) {  // ticket base out of step with the device counter
@@ -234,15 +238,24 @@ __global__ void __launch_bounds__(kHeavyBlock) k_explore_heavy(GraphView g, Heav
 
 // Warp per candidate mu of u: mu stays only if every target v has a
 // candidate among mu's neighbours.
+// True when no target's candidate set changed since u's previous refinement.
+__device__ __forceinline__ bool refine_is_noop(const RefineStamp& rs, const uint32_t* tgt, uint32_t ntgt) {
+  if (rs.prev == 0) return false;
+  for (uint32_t t = 0; t < ntgt; ++t)
+    if (rs.stamp[tgt[2 * t]] >= rs.prev) return false;
+  return true;
+}
+
 __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __restrict__ list,
                                                 const uint32_t* __restrict__ count, uint32_t u,
                                                 const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                 uint32_t* __restrict__ bm, uint32_t words,
-                                                const uint32_t* __restrict__ flags, HeavyList hl) {
+                                                const uint32_t* __restrict__ flags, HeavyList hl, RefineStamp rs) {
   extern __shared__ uint32_t s_tgt[];  // 2 * ntgt: x, label
   for (uint32_t i = threadIdx.x; i < 2 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
   if (*flags & DF_EMPTY) return;
+  if (refine_is_noop(rs, s_tgt, ntgt)) return;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t n = *count;
@@ -269,7 +282,10 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
         }
       }
       if (!found) {
-        if (lane == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        if (lane == 0) {
+          atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+          if (rs.stamp) rs.stamp[u] = rs.seq;
+        }
         break;
       }
     }
@@ -279,8 +295,9 @@ __global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __r
 __global__ void __launch_bounds__(kHeavyBlock) k_refine_heavy(GraphView g, HeavyList hl, uint32_t u,
                                                               const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                               uint32_t* __restrict__ bm, uint32_t words,
-                                                              const uint32_t* __restrict__ flags) {
+                                                              const uint32_t* __restrict__ flags, RefineStamp rs) {
   if (*flags & DF_EMPTY) return;
+  if (refine_is_noop(rs, tgt, ntgt)) return;
   const uint32_t n = min(*hl.count, hl.cap);
   uint32_t* bmu = bm + (size_t)u * words;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
@@ -301,7 +318,10 @@ __global__ void __launch_bounds__(kHeavyBlock) k_refine_heavy(GraphView g, Heavy
         found = __syncthreads_or(hit);
       }
       if (!found) {
-        if (threadIdx.x == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        if (threadIdx.x == 0) {
+          atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+          if (rs.stamp) rs.stamp[u] = rs.seq;
+        }
         break;
       }
     }
@@ -546,10 +566,11 @@ void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint
 }
 
 void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t* list, uint32_t* rank,
-                    uint32_t* count, bool set_empty_flag) {
+                    uint32_t* count, bool set_empty_flag, const uint32_t* stamp, uint32_t u, uint32_t prev) {
   uint32_t tiles = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
   Lookback lb = make_lb(ws, tiles);
-  k_compact<<<tiles, kCompactBlock, 0, ws.stream>>>(bm, words, list, rank, count, lb, set_empty_flag ? 1u : 0u);
+  k_compact<<<tiles, kCompactBlock, 0, ws.stream>>>(bm, words, list, rank, count, lb, set_empty_flag ? 1u : 0u,
+                                                     stamp, u, prev);
   GPSM_LAUNCHED();
 }
 
@@ -579,15 +600,17 @@ void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, c
 }
 
 void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
+                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm,
+                   RefineStamp rs) {
   if (ntgt == 0 || max_count == 0) return;
   HeavyList hl = heavy_list(ws, g);
   uint32_t blocks = grid_for(max_count, 148 * 16);
   k_refine<<<blocks, 256, 2 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
-                                                               ws.d_flags, hl);
+                                                               ws.d_flags, hl, rs);
   GPSM_LAUNCHED();
   if (hl.items) {
-    k_refine_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags);
+    k_refine_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags,
+                                                                  rs);
     GPSM_LAUNCHED();
   }
 }

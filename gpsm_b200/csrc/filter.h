@@ -41,13 +41,29 @@ struct CedgeDir {
   unsigned long long item_base;  // first work item (index into counts/offsets)
 };
 
+// Refinement bookkeeping for skipping exact no-ops: every refine launch has
+// a sequence number (seq, from 1); a launch that removes a candidate of u
+// writes stamp[u] = seq. A refinement of u changes nothing when no target's
+// candidate set changed since u's previous refinement (prev): one pass
+// leaves every remaining candidate with a neighbour in every target's set.
+struct RefineStamp {
+  uint32_t* stamp = nullptr;  // [n] device, zero at query start
+  uint32_t prev = 0;          // seq of u's previous refinement (0: none, run)
+  uint32_t seq = 0;           // this launch
+};
+
 void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint32_t end, uint32_t* bm);
+// stamp/u/prev (optional): skip when C(u) has not changed since the
+// compaction that ran when the last refine seq was `prev` (list and count
+// are still current).
 void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t* list, uint32_t* rank,
-                    uint32_t* count, bool set_empty_flag);
+                    uint32_t* count, bool set_empty_flag, const uint32_t* stamp = nullptr, uint32_t u = 0,
+                    uint32_t prev = 0);
 void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
                     uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
 void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
+                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm,
+                   RefineStamp rs = RefineStamp());
 // d_base[ndir+1]: first work item of each direction, d_base[ndir] = items
 void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
                         const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt);

@@ -249,7 +249,7 @@ int gpsm_match_batch_parallel(gpsm_graph_t g, uint32_t nq, const uint32_t* q_vof
 typedef struct gpsm_server_s* gpsm_server_t;
 typedef struct gpsm_request_info {
   int32_t status;          /* GPSM_OK or an error */
-  int32_t capped;
+  int32_t capped;          /* 1 the embedding cap stopped it, 2 opts->work_cap did */
   uint64_t rows;
   double submit_ms, start_ms, admit_ms, end_ms;  /* server clock */
   double device_ms;

@@ -2,7 +2,7 @@
 
     python -m gpsm_b200.serve_bench [--scale 24] [--rates 200,500,2000] [--requests 1000]
                                     [--slots 8] [--budget-gb 60] [--cap 1000000] [--order learned]
-                                    [--work-cap 2000000000]
+                                    [--work-cap 2000000000] [--slot-arena-gb 16]
 
 Graph: R-MAT(.57,.19,.19,.05) on 2^scale vertices with 16 * 2^scale
 undirected edges (2^24: 256 Mi edges, a 2 GiB int32 CSR), labels Zipf(1.0)
@@ -36,6 +36,8 @@ def main():
     ap.add_argument("--order", default="learned", choices=["plain", "learned"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--work-cap", type=int, default=2_000_000_000)
+    ap.add_argument("--slot-arena-gb", type=float, default=16.0,
+                    help="workspace per slot (filter products, join levels, result buffer)")
     args = ap.parse_args()
     init(0)
     t0 = time.time()
@@ -51,7 +53,7 @@ def main():
         model = L.load(0)
     qs = W.query_set(g, args.requests, W._mix(args.seed, 16), ("geometric", 4, 99), "tree_dense", 0.3, mean=16)
     budget = int(args.budget_gb * (1 << 30))
-    slot_arena = min(16 << 30, budget // args.slots)
+    slot_arena = int(args.slot_arena_gb * (1 << 30))
     for rate in [float(r) for r in args.rates.split(",")]:
         srv = Server(dg, slots=args.slots, memory_budget=budget, slot_arena=slot_arena, cap=args.cap,
                      order=args.order, model=model, work_cap=args.work_cap)

@@ -255,6 +255,8 @@ struct Server {
           mo.admit_ctx = &ctx;
           mo.collect_rows = collect;
           rc = run_query(*ws[s], *g, Q, mo, R);
+        } else {
+          set_last_error(err);
         }
       } catch (const CudaError& e) {
         rc = e.err == cudaErrorMemoryAllocation ? GPSM_ERR_NOMEM : GPSM_ERR_CUDA;

@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict
   }
 }
 
-// Blocks of k_extend one SM holds at once (registers and shared memory
+// Blocks of k_extend_check one SM holds at once (registers and shared memory
 // decide it); asked once per process.
 static uint32_t ext_resident_per_sm() {
   static const uint32_t n = [] {

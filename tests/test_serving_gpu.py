@@ -58,3 +58,19 @@ def test_admission_keeps_join_memory_within_budget(gpu, mixed):
     # latencies are ordered: submit <= start <= admit <= end
     for i in infos:
         assert i["submit_ms"] <= i["start_ms"] <= i["admit_ms"] <= i["end_ms"]
+
+
+def test_failed_request_reports_the_engine_error(gpu, mixed):
+    """A request the engine rejects (a disconnected query) comes back with
+    its status and the engine's error text; the other requests are served."""
+    g, qs, dg = mixed
+    srv = gpu.Server(dg, slots=2, cap=1000, work_cap=10**9)
+    bad = W.Query(np.array([1, 1, 1], np.uint32), np.array([[0, 1]], np.uint32))
+    tb = srv.submit(bad)
+    tg = srv.submit(qs[0])
+    info = srv.wait(tb, raise_on_error=False)
+    assert info["status"] < 0 and "connected" in info["error"]
+    assert srv.wait(tg)["status"] == 0
+    with pytest.raises(gpu.GpsmError):
+        srv.wait(srv.submit(bad))
+    srv.close()

@@ -371,14 +371,27 @@ __global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict
     if (c == 0 || o >= out_cap) continue;
     const uint2* kt = kept + (unsigned long long)tile * kExtTile;
     if (rpw) {
-      // each warp writes rpw whole rows per step: one contiguous span
-      for (uint32_t qb = wid * rpw; qb < c; qb += nwarps * rpw) {
-        const uint32_t q = qb + lane_q;
-        if (lane_on && q < c && o + q < out_cap) {
-          const uint2 e = __ldg(kt + q);
-          out[(o + q) * out_cols + lane_c] =
-              (lane_c < cols) ? __ldg(in + (row_begin + e.x) * cols + lane_c) : e.y;
+      // each warp writes rpw whole rows per step (one contiguous span), four
+      // steps at a time: all loads are issued before the stores, so a lane
+      // has four kept pairs and then four input words in flight
+      constexpr int kU = 4;
+      const uint32_t stride = nwarps * rpw;
+      for (uint32_t qb = wid * rpw; qb < c; qb += kU * stride) {
+        uint2 e[kU];
+        bool on[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const uint32_t q = qb + u * stride + lane_q;
+          on[u] = lane_on && q < c && o + q < out_cap;
+          e[u] = on[u] ? __ldg(kt + q) : make_uint2(0u, 0u);
         }
+        uint32_t val[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          val[u] = (on[u] && lane_c < cols) ? __ldg(in + (row_begin + e[u].x) * cols + lane_c) : e[u].y;
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          if (on[u]) out[(o + qb + u * stride + lane_q) * out_cols + lane_c] = val[u];
       }
       continue;
     }

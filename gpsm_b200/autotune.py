@@ -2,16 +2,18 @@
 
     python -m gpsm_b200.autotune [--workload rmat20] [--queries 24] [--out gpsm_b200/data/tuning.json]
 
-Times a sample of the workload's queries (device time of the whole batch,
-best of two runs after a warm-up) under every combination of:
+Times a sample of the workload's queries in the learned join order (device
+time of the whole batch, best of two runs after a warm-up) under every
+combination of:
   heavy_degree       candidates above it get a block each (filter kernels)
-  ext_blocks_per_sm  persistent join-extend blocks per SM
+  ext_blocks_per_sm  persistent join-check blocks per SM (at most what the
+                     SM holds: 6 at 38 registers a thread)
   step_cands         candidates one join step may admit
   slots              engine slots running queries at once
 and writes the fastest combination to --out; gpsm_b200.init() applies it.
-Queries whose plain-order joins blow up are left out of the sample (they
-measure the order, not the launch shapes): the sample keeps queries whose
-device time under the default choices is below --max-ms.
+Queries that blow up in any order are left out of the sample (they measure
+the order, not the launch shapes): the sample keeps queries whose device
+time under the default choices is below --max-ms.
 """
 import argparse
 import itertools
@@ -22,10 +24,11 @@ import time
 import numpy as np
 
 from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
+from . import learned as L
 from . import workloads as W
 
-GRID = dict(heavy_degree=[256, 1024, 4096], ext_blocks_per_sm=[4, 8], step_cands=[1 << 23, 1 << 25],
-            slots=[1, 2, 4, 8])
+GRID = dict(heavy_degree=[256, 1024, 4096], ext_blocks_per_sm=[3, 6], step_cands=[1 << 23, 1 << 25],
+            slots=[2, 4, 8])
 
 
 def main():
@@ -41,9 +44,10 @@ def main():
     default = get_tuning()
     wl = W.workload(args.workload, count=max(args.queries * 3, 100))
     dg = DeviceGraph(wl.graph)
+    model = L.load(0)
     sample = []
     for q in wl.queries:
-        out = match(dg, q, cap=args.cap, count_only=True)
+        out = match(dg, q, cap=args.cap, count_only=True, order="learned", model=model, work_cap=2_000_000_000)
         if out.info["device_ms"] < args.max_ms:
             sample.append(q)
         if len(sample) >= args.queries:
@@ -53,8 +57,11 @@ def main():
     for combo in itertools.product(*[GRID[k] for k in keys]):
         choice = dict(zip(keys, combo))
         set_tuning(**choice)
-        match_batch(dg, sample, cap=args.cap, slots=choice["slots"])  # warm-up
-        best = min(match_batch(dg, sample, cap=args.cap, slots=choice["slots"])[3]["device_ms"] for _ in range(2))
+        def run():
+            return match_batch(dg, sample, cap=args.cap, slots=choice["slots"], orders="learned", model=model)
+
+        run()  # warm-up
+        best = min(run()[3]["device_ms"] for _ in range(2))
         results.append(dict(choice=choice, device_ms=best))
         print(json.dumps(results[-1]), flush=True)
     set_tuning(**default)

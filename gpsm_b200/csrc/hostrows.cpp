@@ -9,7 +9,10 @@
 // no bounce copy, no page faults: the block was touched and pinned when the
 // pool grew). The caller gets the block itself, and gpsm_free gives it back
 // to the pool, so the next request reuses it. The pool pins at most
-// GPSM_HOST_POOL_GB (default 8) GiB; past that, queries use the other path.
+// GPSM_HOST_POOL_GB GiB (default: a quarter of the host's memory, at most
+// 64 GiB); past that, queries use the other path. A serving loop needs
+// blocks for every finished request its client has not collected yet:
+// requests finish out of order, so that can be many more than the slots.
 //
 // Malloc'd: rows go through two pinned staging buffers per workspace (the
 // DMA of one chunk overlaps the host copy of the previous one) into a
@@ -38,8 +41,13 @@ struct HostPool {
   uint64_t pinned = 0;
   uint64_t limit = 0;
   HostPool() {
-    const char* e = getenv("GPSM_HOST_POOL_GB");
-    limit = (uint64_t)((e ? atof(e) : 8.0) * (double)(1ull << 30));
+    if (const char* e = getenv("GPSM_HOST_POOL_GB")) {
+      limit = (uint64_t)(atof(e) * (double)(1ull << 30));
+    } else {
+      const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
+      const uint64_t phys = pages > 0 && page > 0 ? (uint64_t)pages * (uint64_t)page : (32ull << 30);
+      limit = std::min<uint64_t>(64ull << 30, phys / 4);
+    }
   }
 };
 
@@ -49,30 +57,41 @@ HostPool& pool() {
 }
 
 // A pinned block of at least `bytes`, or null when the pool is at its limit
-// or pinning fails (the caller then uses malloc'd memory).
+// or pinning fails (the caller then uses malloc'd memory). A new block is
+// touched and pinned outside the pool's lock (its size is reserved against
+// the limit first), so other slots keep taking and returning blocks.
 void* pool_acquire(uint64_t bytes, uint64_t* cap) {
   HostPool& P = pool();
-  std::lock_guard<std::mutex> lk(P.mu);
-  auto it = P.free_blocks.lower_bound(bytes);
-  if (it != P.free_blocks.end() && it->first <= 2 * bytes + (64ull << 20)) {
-    void* b = it->second;
-    *cap = it->first;
-    P.free_blocks.erase(it);
-    return b;
-  }
   // size classes: multiples of 64 MiB
   const uint64_t size = (bytes + (64ull << 20) - 1) & ~((64ull << 20) - 1);
-  if (P.pinned + size > P.limit) return nullptr;
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.free_blocks.lower_bound(bytes);
+    if (it != P.free_blocks.end() && it->first <= 2 * bytes + (64ull << 20)) {
+      void* b = it->second;
+      *cap = it->first;
+      P.free_blocks.erase(it);
+      return b;
+    }
+    if (P.pinned + size > P.limit) return nullptr;
+    P.pinned += size;
+  }
   void* b = nullptr;
-  if (posix_memalign(&b, 2ull << 20, size) != 0) return nullptr;
-  madvise(b, size, MADV_HUGEPAGE);
-  memset(b, 0, size);  // fault the pages in now, once
-  if (cudaHostRegister(b, size, cudaHostRegisterDefault) != cudaSuccess) {
-    cudaGetLastError();
-    free(b);
+  bool ok = posix_memalign(&b, 2ull << 20, size) == 0;
+  if (ok) {
+    madvise(b, size, MADV_HUGEPAGE);
+    memset(b, 0, size);  // fault the pages in now, once
+    ok = cudaHostRegister(b, size, cudaHostRegisterDefault) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      free(b);
+    }
+  }
+  std::lock_guard<std::mutex> lk(P.mu);
+  if (!ok) {
+    P.pinned -= size;
     return nullptr;
   }
-  P.pinned += size;
   P.owned[b] = size;
   *cap = size;
   return b;

@@ -947,9 +947,9 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       if (final_level && opt.directed && written) {
         launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
                                res_buf + res_used * qn, d_kept);
-        GPSM_CUDA(cudaMemcpyAsync(&h_st->pad, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        GPSM_CUDA(cudaMemcpyAsync(&h_st->verified, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         GPSM_CUDA(cudaStreamSynchronize(s));
-        kept = std::min<uint64_t>(h_st->pad, cap - emitted);  // the cap counts rows that pass
+        kept = std::min<uint64_t>(h_st->verified, cap - emitted);  // the cap counts rows that pass
         ++exp_launches;
       }
       R.stats.level_rows[lv + 1] += written;

@@ -92,9 +92,8 @@ struct StepState {
   unsigned long long rows;         // input rows admitted (a prefix of the step's rows)
   unsigned long long written;      // output rows written (<= out_cap)
   unsigned long long next_tile;    // tile counter of the check pass
-  unsigned long long unused;
   unsigned long long cands;        // candidates of the admitted rows
-  unsigned long long pad;
+  unsigned long long verified;     // directed mode: rows that passed the verify filter (host copy)
   unsigned long long cand_end;     // end offset of the last admitted row's candidates
   unsigned long long full;         // a row failed admission: later locate tiles skip their rows
 };
@@ -125,6 +124,5 @@ uint64_t join_cands_per_extend_tile();
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj);
-uint64_t join_rows_per_locate_tile();
 
 }  // namespace gpsm

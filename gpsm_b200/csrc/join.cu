@@ -451,7 +451,6 @@ static Lookback next_lb(Workspace& ws, uint64_t tiles) {
   return lb;
 }
 
-uint64_t join_rows_per_locate_tile() { return kLocBlock; }
 uint64_t join_cands_per_extend_tile() { return kExtTile; }
 
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,

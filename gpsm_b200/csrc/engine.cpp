@@ -403,21 +403,27 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   return std::vector<int32_t>(order, order + Q.n);
 }
 
-int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R) {
-  R = MatchResult();
+namespace {
+// Products of the filter phase that the joins read.
+struct FilterProducts {
+  uint32_t* bm = nullptr;              // candidate bitmaps, one per query vertex
+  uint32_t* rank = nullptr;            // per-word ranks of the final lists
+  std::vector<uint32_t*> list;         // final sorted candidate lists
+  std::vector<uint32_t> cnt;           // |C(u)|
+  std::vector<CedgeDir> dirs;          // candidate-edge directions (2 per query edge)
+  unsigned long long* goff = nullptr;  // candidate-edge list offsets
+  uint32_t* nbrs = nullptr;            // candidate-edge lists
+  uint64_t nbrs_total = 0;
+};
+}  // namespace
+
+// Candidate initialisation, exploration, refinement, the final candidate
+// lists with ranks and the candidate edges of every query edge in both
+// directions (match/Match.cu:661-1139). On return R.empty_filter says the
+// query has no embedding (a label is absent or a candidate set ran empty).
+static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, MatchResult& R, FilterProducts& F) {
   const uint32_t qn = Q.n, W = g.words;
   cudaStream_t s = ws.stream;
-  if (ws.dirty) {
-    // an earlier query stopped part-way: re-read the scan ticket counter so
-    // the host's per-launch ticket base matches the device again
-    GPSM_CUDA(cudaStreamSynchronize(s));
-    GPSM_CUDA(cudaMemcpy(&ws.scan.ticket_base, ws.scan.d_ticket, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-  }
-  ws.dirty = true;
-  ws.arena.reset();
-  R.cols = qn;
-  GPSM_CUDA(cudaEventRecord(ws.ev0, s));
-  GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, 64 * sizeof(uint32_t), s));
 
   // ---- allocations ---------------------------------------------------------
   uint32_t* bm = arena_alloc<uint32_t>(ws, (uint64_t)qn * W);
@@ -537,7 +543,6 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small, counts, qn * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 64, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaStreamSynchronize(s));
-  R.stats.filter_launches = launches;
   std::vector<uint32_t> cnt(qn);
   memcpy(cnt.data(), ws.h_small, qn * sizeof(uint32_t));
   const uint32_t flags = *reinterpret_cast<uint32_t*>(ws.h_small + 64);
@@ -614,6 +619,378 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     R.stats.size_fwd[e] = dir_total[2 * e];
     R.stats.size_rev[e] = dir_total[2 * e + 1];
   }
+  R.stats.filter_launches = launches;
+  F.bm = bm;
+  F.rank = rank;
+  F.list = std::move(list);
+  F.cnt = std::move(cnt);
+  F.dirs = std::move(dirs);
+  F.goff = goff;
+  F.nbrs = nbrs;
+  F.nbrs_total = nbrs_total;
+  return GPSM_OK;
+}
+
+// What one join attempt reads and accumulates.
+struct JoinContext {
+  Workspace& ws;
+  const DeviceGraph& g;
+  const QueryPlan& Q;
+  const MatchOptions& opt;
+  MatchResult& R;
+  const FilterProducts& F;
+  const std::vector<int32_t>& pos2id;
+  size_t join_mark;          // arena position where join memory starts
+  uint64_t exp_launches = 0;  // over all attempts
+  uint64_t alg_bytes = 0;
+};
+
+// One attempt joins in the order pos2id until the embeddings are complete,
+// the cap is reached or `limit` candidates have been scanned (limit 0: no
+// limit); hit_limit reports the last. Every attempt starts from the same
+// filter products: it takes join memory from join_mark on and resets the
+// result state.
+static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
+  Workspace& ws = C.ws;
+  const DeviceGraph& g = C.g;
+  const QueryPlan& Q = C.Q;
+  const MatchOptions& opt = C.opt;
+  MatchResult& R = C.R;
+  const std::vector<int32_t>& pos2id = C.pos2id;
+  const size_t join_mark = C.join_mark;
+  uint64_t& exp_launches = C.exp_launches;
+  uint64_t& alg_bytes = C.alg_bytes;
+  const uint32_t qn = Q.n, W = g.words;
+  cudaStream_t s = ws.stream;
+  uint32_t* rank = C.F.rank;
+  const std::vector<uint32_t*>& list = C.F.list;
+  const std::vector<uint32_t>& cnt = C.F.cnt;
+  const std::vector<CedgeDir>& dirs = C.F.dirs;
+  unsigned long long* goff = C.F.goff;
+  uint32_t* nbrs = C.F.nbrs;
+  const uint64_t nbrs_total = C.F.nbrs_total;
+  auto bm_of = [&](uint32_t u) { return C.F.bm + (size_t)u * W; };
+  hit_limit = false;
+  ws.arena.used = join_mark;
+  R.pos2id = pos2id;
+  R.id2pos.assign(qn, -1);
+  for (uint32_t p = 0; p < qn; ++p) R.id2pos[pos2id[p]] = (int32_t)p;
+  R.host_rows.clear();
+  R.d_rows = nullptr;
+  R.d_rows_count = 0;
+  // a capped query that returns its rows gets a page-locked block for all
+  // of them up front: the device copies into it without a bounce buffer
+  if (opt.collect_rows && !opt.keep_on_device && opt.cap != ~0ULL)
+    R.host_rows.reserve_pinned(opt.cap * (uint64_t)qn);
+  // back-neighbour descriptors for each added position p >= 1
+  std::vector<BackNbr> hb;
+  std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
+  // first estimate of candidates per row when extending to position p: the
+  // shortest average candidate-edge list among the placed neighbours (the
+  // driver is the shortest list of each row); later steps use what they saw
+  std::vector<double> ratio0(qn + 1, 4.0);
+  for (uint32_t p = 1; p < qn; ++p) {
+    back_off[p] = (uint32_t)hb.size();
+    const uint32_t v = (uint32_t)pos2id[p];
+    double est = -1.0;
+    for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
+      const uint32_t w = Q.rcol[k];
+      if ((uint32_t)R.id2pos[w] >= p) continue;
+      const int e = Q.edge_between(w, v);
+      const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
+      const double avg = (double)((d & 1) ? R.stats.size_rev[e] : R.stats.size_fwd[e]) /
+                         (double)std::max<uint32_t>(cnt[w], 1);
+      if (est < 0 || avg < est) est = avg;
+      BackNbr b;
+      b.col = (uint32_t)R.id2pos[w];
+      b.pad = 0;
+      b.bm = bm_of(w);
+      b.rank = rank + (size_t)w * W;
+      b.off = goff + dirs[d].item_base;
+      b.nbrs = nbrs;
+      hb.push_back(b);
+      back_cnt[p]++;
+    }
+    if (est >= 0) ratio0[p] = std::max(est, 1.0 / 1024.0);
+  }
+  BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
+  if (!hb.empty())
+    GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
+  // per position: earlier columns holding a query vertex with the same label
+  std::vector<uint32_t> inj, inj_off(qn + 1, 0), inj_cnt(qn, 0);
+  for (uint32_t p = 1; p < qn; ++p) {
+    inj_off[p] = (uint32_t)inj.size();
+    for (uint32_t c = 0; c < p; ++c)
+      if (Q.lab[pos2id[c]] == Q.lab[pos2id[p]]) {
+        inj.push_back(c);
+        inj_cnt[p]++;
+      }
+  }
+  uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
+  if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
+  StepState* d_st = arena_alloc<StepState>(ws, 1);
+  StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
+  JoinScratch js;
+  uint32_t max_nb = 1;
+  for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
+  // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
+  js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
+  js.rng_entries = js.rows * max_nb;
+  js.drv = arena_alloc<uint4>(ws, js.rows);
+  js.rng = arena_alloc<uint4>(ws, js.rng_entries);
+  js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
+  js.tiles = (opt.step_cands + join_cands_per_extend_tile() - 1) / join_cands_per_extend_tile() + 2;
+  js.tile_row = arena_alloc<uint32_t>(ws, js.tiles);
+  js.kept = arena_alloc<uint2>(ws, js.tiles * join_cands_per_extend_tile());
+  js.tile_cnt = arena_alloc<uint32_t>(ws, js.tiles);
+  js.tile_off = arena_alloc<unsigned long long>(ws, js.tiles + 1);
+  GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
+
+  R.stats.level_rows.assign(qn + 1, 0);
+  R.stats.level_in.assign(qn + 1, 0);
+  R.stats.level_cands.assign(qn + 1, 0);
+  uint64_t cands_total = 0;
+  const uint64_t cap = opt.cap;
+  // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
+  std::vector<Level> L(qn + 1);
+  for (uint32_t w = 1; w < qn; ++w) L[w].ratio = ratio0[w];
+  L[1].buf = list[pos2id[0]];
+  L[1].nrows = cnt[pos2id[0]];
+  L[1].cap_rows = L[1].nrows;
+  R.stats.level_rows[1] = L[1].nrows;
+  const uint64_t min_rows = (uint64_t)g.max_degree + 64;
+  const uint64_t lb = level_buffer_bytes(ws, opt, qn);
+  for (uint32_t w = 2; w < qn; ++w) {
+    uint64_t rows = std::max<uint64_t>(lb / (4ull * w), min_rows);
+    L[w].cap_rows = rows;
+    L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
+  }
+  uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
+  if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
+  uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
+  // directed mode: final rows land in a staging buffer and only those whose
+  // query edges are directed, labelled data edges move to the result
+  uint32_t* stage = nullptr;
+  uint64_t stage_rows = 0;
+  uint32_t* d_checks = nullptr;
+  unsigned long long* d_kept = nullptr;
+  uint32_t nchecks = 0;
+  if (opt.directed) {
+    if (!g.dir_off) {
+      set_last_error("directed mode needs gpsm_graph_set_directed");
+      return GPSM_ERR_STATE;
+    }
+    stage_rows = std::max<uint64_t>(opt.level_bytes / (4ull * qn), min_rows);
+    stage = arena_alloc<uint32_t>(ws, stage_rows * qn);
+    std::vector<uint32_t> chk;
+    for (uint32_t k = 0; k < Q.m; ++k) {  // every query edge a -> b (file order) with its label
+      chk.push_back((uint32_t)R.id2pos[Q.fe_from[k]]);
+      chk.push_back((uint32_t)R.id2pos[Q.fe_to[k]]);
+      chk.push_back(k < opt.edge_labels.size() ? opt.edge_labels[k] : 1u);
+    }
+    nchecks = (uint32_t)(chk.size() / 3);
+    d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
+    d_kept = arena_alloc<unsigned long long>(ws, 1);
+    if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+  }
+  uint64_t res_used = 0, emitted = 0;
+  bool capped = false;
+
+  auto flush = [&]() {
+    if (!opt.collect_rows || res_used == 0) {
+      res_used = 0;
+      return;
+    }
+    R.host_rows.append_from_device(ws, res_buf, res_used * qn);
+    res_used = 0;
+  };
+
+  if (qn == 1) {
+    // single-vertex query: every candidate is an embedding
+    const uint64_t n1 = std::min<uint64_t>(L[1].nrows, cap);
+    capped = L[1].nrows >= cap;
+    if (n1 > 0)
+      GPSM_CUDA(cudaMemcpyAsync(res_buf, L[1].buf, std::min(n1, res_cap) * 4, cudaMemcpyDeviceToDevice, s));
+    if (n1 > res_cap) {
+      if (opt.keep_on_device) {
+        set_last_error("device result buffer full");
+        return GPSM_ERR_BUDGET;
+      }
+      if (opt.collect_rows) {
+        R.host_rows.clear();
+        R.host_rows.append_from_device(ws, L[1].buf, n1);
+      }
+    } else {
+      res_used = n1;
+    }
+    emitted = n1;
+    R.stats.level_rows[1] = n1;
+  }
+  while (qn > 1 && !capped) {
+    // deepest level with rows left
+    int lv = -1;
+    for (int w = (int)qn - 1; w >= 1; --w)
+      if (L[w].next < L[w].nrows) {
+        lv = w;
+        break;
+      }
+    if (lv < 0) break;
+    Level& A = L[lv];
+    const bool final_level = (uint32_t)lv + 1 == qn;
+    uint32_t* out;
+    uint64_t out_cap, budget;
+    bool partial = false;
+    if (final_level && opt.directed) {
+      uint64_t space = res_cap - res_used;
+      if (space == 0) {
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        flush();
+        space = res_cap;
+      }
+      out = stage;
+      out_cap = std::min<uint64_t>(stage_rows, space);
+      budget = std::min<uint64_t>(out_cap, opt.step_cands);
+    } else if (final_level) {
+      uint64_t space = res_cap - res_used;
+      if (!opt.keep_on_device && res_used > 0 && cap - emitted > space &&
+          space < std::min<uint64_t>(res_cap, opt.step_cands) / 2) {
+        flush();  // a step into the little space left would be a small one
+        space = res_cap;
+      }
+      out = res_buf + res_used * qn;
+      if (cap - emitted <= space) {
+        // the cap ends the query inside this buffer: rows past it are cut
+        out_cap = cap - emitted;
+        partial = true;
+        budget = std::min<uint64_t>(std::max<uint64_t>(out_cap, min_rows), opt.step_cands);
+      } else {
+        out_cap = space;
+        budget = std::min<uint64_t>(space, opt.step_cands);
+      }
+    } else {
+      Level& B = L[lv + 1];
+      B.nrows = 0;
+      B.next = 0;
+      out = B.buf;
+      out_cap = B.cap_rows;
+      budget = std::min<uint64_t>(out_cap, opt.step_cands);
+    }
+    // rows offered to this step: enough to fill the budget at the observed
+    // candidates per row, within the per-row scratch
+    uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
+    want = std::min<uint64_t>(want, js.rows);
+    const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
+    GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
+    GPSM_CUDA(cudaEventRecord(ws.eve0, s));
+    launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
+                     out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
+    GPSM_CUDA(cudaEventRecord(ws.eve1, s));
+    exp_launches += 4;  // locate, check, scan, write
+    ++R.stats.join_steps;
+    GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    {
+      float ems = 0;
+      GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
+      R.stats.expand_ms += ems;
+    }
+    const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
+    if (trace_enabled()) {
+      float ems = 0;
+      cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
+      const unsigned long long ab = admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull +
+                                    written * 4ull * (lv + 1);
+      fprintf(stderr,
+              "[gpsm] step level=%d nb=%u rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu "
+              "alg_bytes=%llu ms=%.3f\n",
+              lv, back_cnt[lv], (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
+              (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ab, ems);
+    }
+    if (admitted == 0) {
+      if (final_level && !partial && res_used > 0) {  // make room and retry
+        if (opt.keep_on_device) {
+          set_last_error("device result buffer full");
+          return GPSM_ERR_BUDGET;
+        }
+        flush();
+        continue;
+      }
+      set_last_error("a single row has more candidates than a join step admits");
+      return GPSM_ERR_BUDGET;
+    }
+    A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
+    A.next = rb + admitted;
+    alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
+    uint64_t kept = written;
+    if (final_level && opt.directed && written) {
+      launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
+                             res_buf + res_used * qn, d_kept);
+      GPSM_CUDA(cudaMemcpyAsync(&h_st->verified, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      GPSM_CUDA(cudaStreamSynchronize(s));
+      kept = std::min<uint64_t>(h_st->verified, cap - emitted);  // the cap counts rows that pass
+      ++exp_launches;
+    }
+    R.stats.level_rows[lv + 1] += written;
+    R.stats.level_in[lv] += admitted;
+    R.stats.level_cands[lv] += cands;
+    cands_total += cands;
+    R.stats.cands_scanned += cands;
+    if (limit && cands_total >= limit) {
+      hit_limit = true;
+      if (final_level) {
+        res_used += kept;
+        emitted += kept;
+      }
+      break;
+    }
+    if (final_level) {
+      res_used += kept;
+      emitted += kept;
+      if (emitted >= cap) capped = true;
+    } else {
+      L[lv + 1].nrows = written;
+    }
+  }
+  if (emitted >= cap) capped = true;
+  R.rows = emitted;
+  R.capped = capped;
+  GPSM_CUDA(cudaEventRecord(ws.ev1, s));
+  if (opt.collect_rows && !opt.keep_on_device) {
+    flush();
+  } else {
+    R.d_rows = res_buf;
+    R.d_rows_count = res_used;
+  }
+  return GPSM_OK;
+}
+
+// One query: filter (run_filter), join order, admission, then join attempts
+// (join_attempt; the learned plan and the plain order take turns when they
+// race).
+int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R) {
+  R = MatchResult();
+  const uint32_t qn = Q.n;
+  cudaStream_t s = ws.stream;
+  if (ws.dirty) {
+    // an earlier query stopped part-way: re-read the scan ticket counter so
+    // the host's per-launch ticket base matches the device again
+    GPSM_CUDA(cudaStreamSynchronize(s));
+    GPSM_CUDA(cudaMemcpy(&ws.scan.ticket_base, ws.scan.d_ticket, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  }
+  ws.dirty = true;
+  ws.arena.reset();
+  R.cols = qn;
+  GPSM_CUDA(cudaEventRecord(ws.ev0, s));
+  GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, 64 * sizeof(uint32_t), s));
+
+  FilterProducts F;
+  int rc = run_filter(ws, g, Q, R, F);
+  if (rc != GPSM_OK || R.empty_filter) return rc;
+  const std::vector<uint32_t>& cnt = F.cnt;
 
   // ---- join order -------------------------------------------------------------
   std::vector<int32_t> pos2id;
@@ -679,317 +1056,11 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   }
 
   // ---- joins ---------------------------------------------------------------------
-  // One attempt joins in the order pos2id until the embeddings are complete,
-  // the cap is reached or `limit` candidates have been scanned (limit 0: no
-  // limit); hit_limit reports the last. Every attempt starts from the same
-  // filter products: it takes join memory from join_mark on and resets the
-  // result state.
-  const size_t join_mark = ws.arena.used;
-  uint64_t exp_launches = 0;  // over all attempts
-  uint64_t alg_bytes = 0;
-  auto join_attempt = [&](uint64_t limit, bool& hit_limit) -> int {
-    hit_limit = false;
-    ws.arena.used = join_mark;
-    R.pos2id = pos2id;
-    R.id2pos.assign(qn, -1);
-    for (uint32_t p = 0; p < qn; ++p) R.id2pos[pos2id[p]] = (int32_t)p;
-    R.host_rows.clear();
-    R.d_rows = nullptr;
-    R.d_rows_count = 0;
-    // a capped query that returns its rows gets a page-locked block for all
-    // of them up front: the device copies into it without a bounce buffer
-    if (opt.collect_rows && !opt.keep_on_device && opt.cap != ~0ULL)
-      R.host_rows.reserve_pinned(opt.cap * (uint64_t)qn);
-    // back-neighbour descriptors for each added position p >= 1
-    std::vector<BackNbr> hb;
-    std::vector<uint32_t> back_off(qn + 1, 0), back_cnt(qn, 0);
-    // first estimate of candidates per row when extending to position p: the
-    // shortest average candidate-edge list among the placed neighbours (the
-    // driver is the shortest list of each row); later steps use what they saw
-    std::vector<double> ratio0(qn + 1, 4.0);
-    for (uint32_t p = 1; p < qn; ++p) {
-      back_off[p] = (uint32_t)hb.size();
-      const uint32_t v = (uint32_t)pos2id[p];
-      double est = -1.0;
-      for (uint32_t k = Q.roff[v]; k < Q.roff[v + 1]; ++k) {
-        const uint32_t w = Q.rcol[k];
-        if ((uint32_t)R.id2pos[w] >= p) continue;
-        const int e = Q.edge_between(w, v);
-        const uint32_t d = 2 * (uint32_t)e + (Q.efrom[e] == w ? 0u : 1u);
-        const double avg = (double)((d & 1) ? R.stats.size_rev[e] : R.stats.size_fwd[e]) /
-                           (double)std::max<uint32_t>(cnt[w], 1);
-        if (est < 0 || avg < est) est = avg;
-        BackNbr b;
-        b.col = (uint32_t)R.id2pos[w];
-        b.pad = 0;
-        b.bm = bm_of(w);
-        b.rank = rank + (size_t)w * W;
-        b.off = goff + dirs[d].item_base;
-        b.nbrs = nbrs;
-        hb.push_back(b);
-        back_cnt[p]++;
-      }
-      if (est >= 0) ratio0[p] = std::max(est, 1.0 / 1024.0);
-    }
-    BackNbr* d_back = arena_alloc<BackNbr>(ws, hb.size() + 1);
-    if (!hb.empty())
-      GPSM_CUDA(cudaMemcpyAsync(d_back, hb.data(), hb.size() * sizeof(BackNbr), cudaMemcpyHostToDevice, s));
-    // per position: earlier columns holding a query vertex with the same label
-    std::vector<uint32_t> inj, inj_off(qn + 1, 0), inj_cnt(qn, 0);
-    for (uint32_t p = 1; p < qn; ++p) {
-      inj_off[p] = (uint32_t)inj.size();
-      for (uint32_t c = 0; c < p; ++c)
-        if (Q.lab[pos2id[c]] == Q.lab[pos2id[p]]) {
-          inj.push_back(c);
-          inj_cnt[p]++;
-        }
-    }
-    uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
-    if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
-    StepState* d_st = arena_alloc<StepState>(ws, 1);
-    StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
-    JoinScratch js;
-    uint32_t max_nb = 1;
-    for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
-    // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
-    js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
-    js.rng_entries = js.rows * max_nb;
-    js.drv = arena_alloc<uint4>(ws, js.rows);
-    js.rng = arena_alloc<uint4>(ws, js.rng_entries);
-    js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
-    js.tiles = (opt.step_cands + join_cands_per_extend_tile() - 1) / join_cands_per_extend_tile() + 2;
-    js.tile_row = arena_alloc<uint32_t>(ws, js.tiles);
-    js.kept = arena_alloc<uint2>(ws, js.tiles * join_cands_per_extend_tile());
-    js.tile_cnt = arena_alloc<uint32_t>(ws, js.tiles);
-    js.tile_off = arena_alloc<unsigned long long>(ws, js.tiles + 1);
-    GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
-
-    R.stats.level_rows.assign(qn + 1, 0);
-    R.stats.level_in.assign(qn + 1, 0);
-    R.stats.level_cands.assign(qn + 1, 0);
-    uint64_t cands_total = 0;
-    const uint64_t cap = opt.cap;
-    // levels 1..qn; level w holds rows of width w. Level 1 is C(pos2id[0]).
-    std::vector<Level> L(qn + 1);
-    for (uint32_t w = 1; w < qn; ++w) L[w].ratio = ratio0[w];
-    L[1].buf = list[pos2id[0]];
-    L[1].nrows = cnt[pos2id[0]];
-    L[1].cap_rows = L[1].nrows;
-    R.stats.level_rows[1] = L[1].nrows;
-    const uint64_t min_rows = (uint64_t)g.max_degree + 64;
-    const uint64_t lb = level_buffer_bytes(ws, opt, qn);
-    for (uint32_t w = 2; w < qn; ++w) {
-      uint64_t rows = std::max<uint64_t>(lb / (4ull * w), min_rows);
-      L[w].cap_rows = rows;
-      L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
-    }
-    uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
-    if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
-    uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
-    // directed mode: final rows land in a staging buffer and only those whose
-    // query edges are directed, labelled data edges move to the result
-    uint32_t* stage = nullptr;
-    uint64_t stage_rows = 0;
-    uint32_t* d_checks = nullptr;
-    unsigned long long* d_kept = nullptr;
-    uint32_t nchecks = 0;
-    if (opt.directed) {
-      if (!g.dir_off) {
-        set_last_error("directed mode needs gpsm_graph_set_directed");
-        return GPSM_ERR_STATE;
-      }
-      stage_rows = std::max<uint64_t>(opt.level_bytes / (4ull * qn), min_rows);
-      stage = arena_alloc<uint32_t>(ws, stage_rows * qn);
-      std::vector<uint32_t> chk;
-      for (uint32_t k = 0; k < Q.m; ++k) {  // every query edge a -> b (file order) with its label
-        chk.push_back((uint32_t)R.id2pos[Q.fe_from[k]]);
-        chk.push_back((uint32_t)R.id2pos[Q.fe_to[k]]);
-        chk.push_back(k < opt.edge_labels.size() ? opt.edge_labels[k] : 1u);
-      }
-      nchecks = (uint32_t)(chk.size() / 3);
-      d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
-      d_kept = arena_alloc<unsigned long long>(ws, 1);
-      if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
-      GPSM_CUDA(cudaStreamSynchronize(s));
-    }
-    uint64_t res_used = 0, emitted = 0;
-    bool capped = false;
-
-    auto flush = [&]() {
-      if (!opt.collect_rows || res_used == 0) {
-        res_used = 0;
-        return;
-      }
-      R.host_rows.append_from_device(ws, res_buf, res_used * qn);
-      res_used = 0;
-    };
-
-    if (qn == 1) {
-      // single-vertex query: every candidate is an embedding
-      const uint64_t n1 = std::min<uint64_t>(L[1].nrows, cap);
-      capped = L[1].nrows >= cap;
-      if (n1 > 0)
-        GPSM_CUDA(cudaMemcpyAsync(res_buf, L[1].buf, std::min(n1, res_cap) * 4, cudaMemcpyDeviceToDevice, s));
-      if (n1 > res_cap) {
-        if (opt.keep_on_device) {
-          set_last_error("device result buffer full");
-          return GPSM_ERR_BUDGET;
-        }
-        if (opt.collect_rows) {
-          R.host_rows.clear();
-          R.host_rows.append_from_device(ws, L[1].buf, n1);
-        }
-      } else {
-        res_used = n1;
-      }
-      emitted = n1;
-      R.stats.level_rows[1] = n1;
-    }
-    while (qn > 1 && !capped) {
-      // deepest level with rows left
-      int lv = -1;
-      for (int w = (int)qn - 1; w >= 1; --w)
-        if (L[w].next < L[w].nrows) {
-          lv = w;
-          break;
-        }
-      if (lv < 0) break;
-      Level& A = L[lv];
-      const bool final_level = (uint32_t)lv + 1 == qn;
-      uint32_t* out;
-      uint64_t out_cap, budget;
-      bool partial = false;
-      if (final_level && opt.directed) {
-        uint64_t space = res_cap - res_used;
-        if (space == 0) {
-          if (opt.keep_on_device) {
-            set_last_error("device result buffer full");
-            return GPSM_ERR_BUDGET;
-          }
-          flush();
-          space = res_cap;
-        }
-        out = stage;
-        out_cap = std::min<uint64_t>(stage_rows, space);
-        budget = std::min<uint64_t>(out_cap, opt.step_cands);
-      } else if (final_level) {
-        uint64_t space = res_cap - res_used;
-        if (!opt.keep_on_device && res_used > 0 && cap - emitted > space &&
-            space < std::min<uint64_t>(res_cap, opt.step_cands) / 2) {
-          flush();  // a step into the little space left would be a small one
-          space = res_cap;
-        }
-        out = res_buf + res_used * qn;
-        if (cap - emitted <= space) {
-          // the cap ends the query inside this buffer: rows past it are cut
-          out_cap = cap - emitted;
-          partial = true;
-          budget = std::min<uint64_t>(std::max<uint64_t>(out_cap, min_rows), opt.step_cands);
-        } else {
-          out_cap = space;
-          budget = std::min<uint64_t>(space, opt.step_cands);
-        }
-      } else {
-        Level& B = L[lv + 1];
-        B.nrows = 0;
-        B.next = 0;
-        out = B.buf;
-        out_cap = B.cap_rows;
-        budget = std::min<uint64_t>(out_cap, opt.step_cands);
-      }
-      // rows offered to this step: enough to fill the budget at the observed
-      // candidates per row, within the per-row scratch
-      uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
-      want = std::min<uint64_t>(want, js.rows);
-      const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
-      GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
-      GPSM_CUDA(cudaEventRecord(ws.eve0, s));
-      launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                       out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
-      GPSM_CUDA(cudaEventRecord(ws.eve1, s));
-      exp_launches += 4;  // locate, check, scan, write
-      ++R.stats.join_steps;
-      GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
-      GPSM_CUDA(cudaStreamSynchronize(s));
-      {
-        float ems = 0;
-        GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
-        R.stats.expand_ms += ems;
-      }
-      const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
-      if (trace_enabled()) {
-        float ems = 0;
-        cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
-        const unsigned long long ab = admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull +
-                                      written * 4ull * (lv + 1);
-        fprintf(stderr,
-                "[gpsm] step level=%d nb=%u rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu "
-                "alg_bytes=%llu ms=%.3f\n",
-                lv, back_cnt[lv], (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
-                (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ab, ems);
-      }
-      if (admitted == 0) {
-        if (final_level && !partial && res_used > 0) {  // make room and retry
-          if (opt.keep_on_device) {
-            set_last_error("device result buffer full");
-            return GPSM_ERR_BUDGET;
-          }
-          flush();
-          continue;
-        }
-        set_last_error("a single row has more candidates than a join step admits");
-        return GPSM_ERR_BUDGET;
-      }
-      A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
-      A.next = rb + admitted;
-      alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
-      uint64_t kept = written;
-      if (final_level && opt.directed && written) {
-        launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
-                               res_buf + res_used * qn, d_kept);
-        GPSM_CUDA(cudaMemcpyAsync(&h_st->verified, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-        GPSM_CUDA(cudaStreamSynchronize(s));
-        kept = std::min<uint64_t>(h_st->verified, cap - emitted);  // the cap counts rows that pass
-        ++exp_launches;
-      }
-      R.stats.level_rows[lv + 1] += written;
-      R.stats.level_in[lv] += admitted;
-      R.stats.level_cands[lv] += cands;
-      cands_total += cands;
-      R.stats.cands_scanned += cands;
-      if (limit && cands_total >= limit) {
-        hit_limit = true;
-        if (final_level) {
-          res_used += kept;
-          emitted += kept;
-        }
-        break;
-      }
-      if (final_level) {
-        res_used += kept;
-        emitted += kept;
-        if (emitted >= cap) capped = true;
-      } else {
-        L[lv + 1].nrows = written;
-      }
-    }
-    if (emitted >= cap) capped = true;
-    R.rows = emitted;
-    R.capped = capped;
-    GPSM_CUDA(cudaEventRecord(ws.ev1, s));
-    if (opt.collect_rows && !opt.keep_on_device) {
-      flush();
-    } else {
-      R.d_rows = res_buf;
-      R.d_rows_count = res_used;
-    }
-    return GPSM_OK;
-  };
-
+  JoinContext ctx{ws, g, Q, opt, R, F, pos2id, ws.arena.used};
   int jrc = GPSM_OK;
   bool hit = false;
   if (race.empty()) {
-    jrc = join_attempt(opt.work_cap, hit);
+    jrc = join_attempt(ctx, opt.work_cap, hit);
     R.stats.aborted = hit;
   } else {
     // the learned plan and the plain order take turns with work shares that
@@ -1003,7 +1074,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       pos2id = learned_turn ? learned_plan : race;
       const bool last = (opt.work_cap && share >= opt.work_cap) || share >= (1ull << 60);
       ++R.stats.order_attempts;
-      jrc = join_attempt(last ? opt.work_cap : share, hit);
+      jrc = join_attempt(ctx, last ? opt.work_cap : share, hit);
       if (jrc != GPSM_OK || !hit || last) {
         R.stats.aborted = hit;
         if (!learned_turn) R.stats.order_fallback = 3;
@@ -1012,8 +1083,8 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
       if (!learned_turn) share *= 4;
     }
   }
-  R.stats.expand_launches = exp_launches;
-  R.stats.alg_bytes_join = alg_bytes;
+  R.stats.expand_launches = ctx.exp_launches;
+  R.stats.alg_bytes_join = ctx.alg_bytes;
   if (jrc != GPSM_OK) return jrc;
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4001, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaEventSynchronize(ws.ev1));

@@ -280,7 +280,7 @@ int gpsm_last_levels(gpsm_engine_t e, uint32_t n, uint64_t* level_in, uint64_t* 
  * match/Match.cu:455, 649, 1313). */
 typedef struct gpsm_tuning {
   uint32_t heavy_degree;       /* candidates with more neighbours: one block each (default 1024) */
-  uint32_t ext_blocks_per_sm;  /* persistent join-extend blocks per SM (1..8, default 8) */
+  uint32_t ext_blocks_per_sm;  /* persistent join-check blocks per SM (1..8, default 8; at most what an SM holds) */
   uint64_t step_cands;         /* candidates one join step may admit (default 2^25) */
   uint64_t level_bytes;        /* bytes per intermediate join level (default 256 MiB) */
   uint32_t slots;              /* engine slots for batches and serving (default 4) */

@@ -549,7 +549,15 @@ int gpsm_select_vertices(gpsm_engine_t eng, const uint32_t* d_labels, const uint
     }
     GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, sizeof(uint32_t), ws.stream));
     select_vertices(ws, d_labels, d_offsets, n, label, min_degree, bm, d_out, d_count);
+    GPSM_CUDA(cudaMemcpyAsync(ws.h_small, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, ws.stream));
     GPSM_CUDA(cudaStreamSynchronize(ws.stream));
+    // a look-back wait that gave up or a ticket out of range leaves the list
+    // and count wrong: report it instead of returning them
+    if (*reinterpret_cast<const uint32_t*>(ws.h_small) & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {
+      set_last_error("gpsm_select_vertices: device wait limit or bounds check tripped");
+      ws.dirty = true;
+      return GPSM_ERR_TIMEOUT;
+    }
     return GPSM_OK;
   });
 }

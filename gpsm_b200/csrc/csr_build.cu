@@ -1,5 +1,5 @@
 // Undirected CSR construction on the device, the job Graph::transformToCSR
-// does on the host (graph/Graph.cpp:190-226; its comment at :187 asks for a
+// does on the host (graph/Graph.cpp:30-65; its comment at :26-27 asks for a
 // GPU version): every undirected edge (u, v) becomes the keys u<<32|v and
 // v<<32|u, an LSD radix sort orders them by (source, target), and the
 // targets in key order are the column array, every list ascending. Offsets

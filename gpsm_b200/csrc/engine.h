@@ -26,8 +26,8 @@ void workspace_free(Workspace* ws);
 struct QueryPlan {
   uint32_t n = 0, m = 0;
   std::vector<uint32_t> lab;
-  std::vector<std::vector<uint32_t>> in, out;  // file-order directed lists (graph/Graph.cpp:180-185)
-  std::vector<uint32_t> roff, rcol;             // undirected CSR, lists sorted (graph/Graph.cpp:190-226)
+  std::vector<std::vector<uint32_t>> in, out;  // file-order directed lists (graph/Graph.cpp:20-24)
+  std::vector<uint32_t> roff, rcol;             // undirected CSR, lists sorted (graph/Graph.cpp:30-65)
   std::vector<uint32_t> efrom, eto;             // edge ids (match/Match.cu:1738-1754), from < to
   std::vector<uint32_t> order;                  // filter order (match/Match.cu:339-429)
   std::vector<uint32_t> fe_from, fe_to;         // edges as given (file order, directed)

@@ -2,8 +2,8 @@
 // uniform and Zipf vertex labels, undirected CSR construction with sorted
 // adjacency, and random-walk query extraction.
 //
-// The reference reads its graphs from text files (io/IO.cpp:87-142) and
-// builds the undirected CSR on the host (graph/Graph.cpp:190-226: in- and
+// The reference reads its graphs from text files (io/IO.cpp:46-128) and
+// builds the undirected CSR on the host (graph/Graph.cpp:30-65: in- and
 // out-lists merged, each list sorted ascending). gpsm_csr_from_edges
 // produces the same arrays from an edge list in which every undirected edge
 // appears once, which is the file convention the reference assumes
@@ -276,7 +276,7 @@ extern "C" int gpsm_gen_labels(uint32_t n, uint32_t num_labels, double zipf_s, u
   return GPSM_OK;
 }
 
-// Undirected CSR with every adjacency list sorted ascending (graph/Graph.cpp:190-226).
+// Undirected CSR with every adjacency list sorted ascending (graph/Graph.cpp:30-65).
 // edges: m pairs (u, v), each undirected edge once. Parallel edges and self
 // loops are kept exactly as given, like the reference.
 extern "C" int gpsm_csr_from_edges(uint32_t n, uint64_t m, const uint32_t* edges, uint32_t* offsets,

@@ -9,6 +9,9 @@
 #include <algorithm>
 #include <cstdio>
 
+// Drops the device copy the drop-in Match uploaded for this graph (host/Match.cpp).
+void gpsm_host_forget_graph(const Graph* g);
+
 void Graph::addVertex(LABEL vlb) { vertices.push_back(Vertex(vlb)); }
 
 void Graph::addEdge(VID from, VID to, LABEL elb) {
@@ -21,6 +24,9 @@ Graph::Graph()
       label_num(0), inverse_label(nullptr), inverse_num(nullptr) {}
 
 Graph::~Graph() {
+  // the reference's driver deletes each data graph (main/run.cpp:97) and the
+  // next one may be allocated at the same address
+  gpsm_host_forget_graph(this);
   delete[] vertex_value;
   delete[] undirected_row_offset;
   delete[] undirected_column_index;
@@ -29,6 +35,7 @@ Graph::~Graph() {
 }
 
 void Graph::transformToCSR() {
+  gpsm_host_forget_graph(this);  // a device copy of the old CSR is stale
   delete[] vertex_value;
   delete[] undirected_row_offset;
   delete[] undirected_column_index;

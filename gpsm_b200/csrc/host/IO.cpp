@@ -106,7 +106,7 @@ bool IO::output() {
 }
 
 // injective, and every query in-edge (src -> i, label) exists as a data
-// out-edge ans[src] -> ans[i] with that label (io/IO.cpp:187-222)
+// out-edge ans[src] -> ans[i] with that label (io/IO.cpp:146-180)
 bool IO::verify(int* id_map, unsigned* ans, unsigned num, Graph* query, Graph* data) {
   std::set<unsigned> seen;
   for (unsigned i = 0; i < num; ++i)

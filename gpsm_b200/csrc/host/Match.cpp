@@ -16,7 +16,15 @@
 
 namespace {
 std::mutex g_mu;
-std::map<Graph*, gpsm_graph_t> g_graphs;  // data graphs already on the device
+// data graphs already on the device, keyed by the Graph object; an entry
+// lives exactly as long as its Graph's CSR (Graph::~Graph and
+// Graph::transformToCSR drop it), so a new Graph that reuses a deleted one's
+// address is uploaded afresh. Never destroyed: a Graph may die after static
+// destructors have run.
+std::map<const Graph*, gpsm_graph_t>& graphs() {
+  static auto* m = new std::map<const Graph*, gpsm_graph_t>();
+  return *m;
+}
 uint64_t g_cap = 0;
 
 void die(const char* what, int rc) {
@@ -25,18 +33,28 @@ void die(const char* what, int rc) {
 }
 
 gpsm_graph_t device_graph(Graph* data) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_graphs.find(data);
-  if (it != g_graphs.end()) return it->second;
   if (!data->undirected_row_offset) data->transformToCSR();
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = graphs().find(data);
+  if (it != graphs().end()) return it->second;
   gpsm_graph_t h = nullptr;
   int rc = gpsm_graph_upload(data->undirected_row_offset, data->undirected_column_index, data->vertex_value,
                              data->vertex_num, &h);
   if (rc != GPSM_OK) die("gpsm_graph_upload", rc);
-  g_graphs[data] = h;
+  graphs()[data] = h;
   return h;
 }
 }  // namespace
+
+// Called by Graph::~Graph and Graph::transformToCSR: the device copy (if any)
+// belongs to the CSR being dropped.
+void gpsm_host_forget_graph(const Graph* g) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = graphs().find(g);
+  if (it == graphs().end()) return;
+  gpsm_graph_free(it->second);
+  graphs().erase(it);
+}
 
 void Match::initGPU(int dev) {
   int rc = gpsm_init(dev);
@@ -49,13 +67,7 @@ void Match::initGPU(int dev) {
 
 void Match::setCap(uint64_t cap) { g_cap = cap; }
 
-void Match::releaseGraph(Graph* data) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_graphs.find(data);
-  if (it == g_graphs.end()) return;
-  gpsm_graph_free(it->second);
-  g_graphs.erase(it);
-}
+void Match::releaseGraph(Graph* data) { gpsm_host_forget_graph(data); }
 
 Match::Match(Graph* q, Graph* d) : query(q), data(d), id2pos(nullptr) {}
 

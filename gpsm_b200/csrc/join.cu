@@ -7,7 +7,7 @@
 // tree edge, join_kernel + filter_kernel drop rows failing a non-tree edge.
 // Each of those kernels finds mu in the candidate list by a warp-wide
 // LINEAR scan of C(u) per row, runs one warp per row whatever the row's
-// list length, and none checks injectivity (io/IO.cpp:187-222 filters on the
+// list length, and none checks injectivity (io/IO.cpp:146-180 filters on the
 // host afterwards).
 //
 // Here a step is four kernels:

@@ -19,7 +19,8 @@
 // code never passes it to a kernel: the first call on each device looks up
 // the device address with cudaGetSymbolAddress (with that device current)
 // and caches it; later calls on that device reuse it. Make that first call
-// before any stream capture. Every call shares the one array and it keeps
+// before any stream capture. Every call reads the error flags back and waits
+// for `stream` to finish before it returns. Every call shares the one array and it keeps
 // the last call's contents, so each call rewrites the whole bitmap and
 // clears the scan state and flags it needs zeroed; two calls that overlap on
 // the GPU (different streams, or host threads racing) corrupt each other.
@@ -113,6 +114,12 @@ extern "C" int gpsm_select_vertices_static(const uint32_t* d_labels, const uint3
     }
   } catch (const CudaError& e) {
     return e.err == cudaErrorInvalidValue ? GPSM_ERR_INVALID : GPSM_ERR_CUDA;
+  } catch (const std::bad_alloc&) {  // nothing may cross the C boundary
+    set_last_error("gpsm_select_vertices_static: host allocation failed");
+    return GPSM_ERR_NOMEM;
+  } catch (...) {
+    set_last_error("gpsm_select_vertices_static: unexpected exception");
+    return GPSM_ERR_STATE;
   }
   return GPSM_OK;
 }

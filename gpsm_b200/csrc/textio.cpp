@@ -1,4 +1,4 @@
-// The reference's graph text format at full speed (io/IO.cpp:87-142 reads
+// The reference's graph text format at full speed (io/IO.cpp:46-128 reads
 // it with one fscanf per token, which takes minutes for a 256M-edge file).
 //
 // Format: `t # <id>` starts a graph (id -1 ends the file), then a line of

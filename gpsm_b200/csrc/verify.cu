@@ -1,5 +1,5 @@
 // Directed, edge-labelled verification on the device (the reference's
-// IO::verify, io/IO.cpp:187-222, which runs on the host per row after the
+// IO::verify, io/IO.cpp:146-180, which runs on the host per row after the
 // undirected match): a row survives when every query edge (a -> b, label l)
 // exists as a data edge row[a] -> row[b] with label l. The engine matches
 // undirected, edge-unlabelled (as the reference's GPU part does), then runs

@@ -15,7 +15,12 @@ available, so every workload is generated from a seed:
                4,096 queries of 4..64 vertices (tree/dense mix)
   rmat24       R-MAT on 2^24 vertices, 256 Mi edges, Zipf(1.0) over 1..128;
                queries of 4..99 vertices, geometric with mean 16
-All generation runs in libgpsm.so (gen.cpp); this module only sequences it.
+Generation runs in compiled code (gen.cpp); this module only sequences it.
+The default source is libgpsm.so (its generators and CSR builder). Test and
+benchmark code that must not load the engine (the CPU reference arm) passes
+oracle.GEN_SOURCE instead: the same generators compiled into liboracle.so,
+with the oracle's own CSR construction; both sources give identical
+workloads (tests/test_oracle.py checks it).
 """
 from dataclasses import dataclass, field
 
@@ -73,37 +78,56 @@ def _mix(a, b):
     return x ^ (x >> 31)
 
 
-def graph_from_edges(n, edges, labels, name=""):
-    lib = _lib.load()
+class Source:
+    """Where workloads are drawn: `lib()` returns a ctypes library exporting
+    gpsm_gen_er / gpsm_gen_rmat / gpsm_gen_labels / gpsm_gen_query, and
+    `csr(n, edges)` returns (offsets, cols)."""
+
+    name = "libgpsm"
+
+    def lib(self):
+        return _lib.load()
+
+    def csr(self, n, edges):
+        lib = _lib.load()
+        m = edges.shape[0]
+        off = np.zeros(n + 1, dtype=np.uint32)
+        cols = np.zeros(max(2 * m, 1), dtype=np.uint32)
+        _lib.check(lib.gpsm_csr_from_edges(n, m, _lib.ptr(edges), _lib.ptr(off), _lib.ptr(cols)), "csr")
+        return off, cols[: 2 * m]
+
+
+ENGINE_SOURCE = Source()
+
+
+def graph_from_edges(n, edges, labels, name="", source=None):
+    source = source or ENGINE_SOURCE
     edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
-    m = edges.shape[0]
-    off = np.zeros(n + 1, dtype=np.uint32)
-    cols = np.zeros(max(2 * m, 1), dtype=np.uint32)
-    _lib.check(lib.gpsm_csr_from_edges(n, m, _lib.ptr(edges), _lib.ptr(off), _lib.ptr(cols)), "csr")
-    return Graph(n, off, cols[: 2 * m], _lib.u32a(labels), edges, name)
+    off, cols = source.csr(n, edges)
+    return Graph(n, off, cols, _lib.u32a(labels), edges, name)
 
 
-def er_graph(n, m, num_labels, seed, zipf_s=0.0, name="er"):
-    lib = _lib.load()
+def er_graph(n, m, num_labels, seed, zipf_s=0.0, name="er", source=None):
+    lib = (source or ENGINE_SOURCE).lib()
     edges = np.zeros((m, 2), dtype=np.uint32)
     _lib.check(lib.gpsm_gen_er(n, m, seed, _lib.ptr(edges)), "gen_er")
     labels = np.zeros(n, dtype=np.uint32)
     _lib.check(lib.gpsm_gen_labels(n, num_labels, zipf_s, _mix(seed, 7), _lib.ptr(labels)), "labels")
-    return graph_from_edges(n, edges, labels, name)
+    return graph_from_edges(n, edges, labels, name, source)
 
 
-def rmat_graph(scale, m, num_labels, zipf_s, seed, a=0.57, b=0.19, c=0.19, name="rmat"):
-    lib = _lib.load()
+def rmat_graph(scale, m, num_labels, zipf_s, seed, a=0.57, b=0.19, c=0.19, name="rmat", source=None):
+    lib = (source or ENGINE_SOURCE).lib()
     edges = np.zeros((m, 2), dtype=np.uint32)
     _lib.check(lib.gpsm_gen_rmat(scale, m, a, b, c, seed, _lib.ptr(edges)), "gen_rmat")
     n = 1 << scale
     labels = np.zeros(n, dtype=np.uint32)
     _lib.check(lib.gpsm_gen_labels(n, num_labels, zipf_s, _mix(seed, 7), _lib.ptr(labels)), "labels")
-    return graph_from_edges(n, edges, labels, name)
+    return graph_from_edges(n, edges, labels, name, source)
 
 
-def random_walk_query(g, qn, seed, mode=MODE_INDUCED, p_extra=0.0, min_avg_degree=0.0):
-    lib = _lib.load()
+def random_walk_query(g, qn, seed, mode=MODE_INDUCED, p_extra=0.0, min_avg_degree=0.0, source=None):
+    lib = (source or ENGINE_SOURCE).lib()
     ql = np.zeros(qn, dtype=np.uint32)
     qe = np.zeros(max(qn * (qn - 1), 2), dtype=np.uint32)
     ids = np.zeros(qn, dtype=np.uint32)
@@ -125,12 +149,13 @@ def _size_stream(rng, kind, count, lo, hi, mean=None):
 
 
 def query_set(g, count, seed, sizes=("fixed", 6, 6), mix="induced", p_extra=0.3,
-              min_avg_degree=0.0, mean=None):
-    """count random-walk queries; mix is 'induced', 'tree', 'dense' or 'tree_dense' (50/50)."""
+              min_avg_degree=0.0, mean=None, source=None, first=0):
+    """Queries first .. count-1 of a seeded set of random-walk queries; mix
+    is 'induced', 'tree', 'dense' or 'tree_dense' (50/50)."""
     rng = np.random.default_rng(_mix(seed, 0x512E))
     qsizes = _size_stream(rng, sizes[0], count, sizes[1], sizes[2], mean)
     out = []
-    for k in range(count):
+    for k in range(first, count):
         qs = _mix(seed, 1000 + k)
         if mix == "induced":
             mode = MODE_INDUCED
@@ -140,60 +165,62 @@ def query_set(g, count, seed, sizes=("fixed", 6, 6), mix="induced", p_extra=0.3,
             mode = MODE_DENSE
         else:
             mode = MODE_TREE if k % 2 == 0 else MODE_DENSE
-        out.append(random_walk_query(g, qsizes[k], qs, mode, p_extra, min_avg_degree))
+        out.append(random_walk_query(g, qsizes[k], qs, mode, p_extra, min_avg_degree, source))
     return out
 
 
 _GRAPH_CACHE = {}
 
+# name -> (generator, args, seed salt)
+_GRAPHS = {
+    "small_er": ("er", (10_000, 40_000, 8), 1),
+    "rmat20": ("rmat", (20, 16 << 20, 32, 1.0), 2),
+    "rmat22": ("rmat", (22, 64 << 20, 64, 1.1), 4),
+    "rmat24": ("rmat", (24, 256 << 20, 128, 1.0), 5),
+}
 
-def graph_for(name, seed=0):
-    key = (name, seed)
+# name -> (graph, default count, seed salt, sizes, mix, p_extra, min_avg_degree, mean)
+_QUERIES = {
+    "small_er": ("small_er", 10, 11, ("fixed", 6, 6), "induced", 0.3, 0.0, None),
+    "rmat20": ("rmat20", 100, 12, ("fixed", 12, 12), "induced", 0.3, 2.5, None),
+    "rmat20_mix": ("rmat20", 1000, 13, ("uniform", 4, 32), "tree_dense", 0.3, 0.0, None),
+    "rmat20_train": ("rmat20", 5000, 14, ("uniform", 4, 32), "tree_dense", 0.3, 0.0, None),
+    "rmat22": ("rmat22", 4096, 15, ("uniform", 4, 64), "tree_dense", 0.3, 0.0, None),
+    "rmat24": ("rmat24", 2000, 16, ("geometric", 4, 99), "tree_dense", 0.3, 0.0, 16),
+}
+
+
+def graph_for(name, seed=0, source=None):
+    source = source or ENGINE_SOURCE
+    key = (name, seed, source.name)
     if key in _GRAPH_CACHE:
         return _GRAPH_CACHE[key]
-    if name == "small_er":
-        g = er_graph(10_000, 40_000, 8, _mix(seed, 1), name=name)
-    elif name == "rmat20":
-        g = rmat_graph(20, 16 << 20, 32, 1.0, _mix(seed, 2), name=name)
-    elif name == "rmat22":
-        g = rmat_graph(22, 64 << 20, 64, 1.1, _mix(seed, 4), name=name)
-    elif name == "rmat24":
-        g = rmat_graph(24, 256 << 20, 128, 1.0, _mix(seed, 5), name=name)
-    else:
+    if name not in _GRAPHS:
         raise ValueError(name)
+    kind, args, salt = _GRAPHS[name]
+    if kind == "er":
+        g = er_graph(*args, _mix(seed, salt), name=name, source=source)
+    else:
+        g = rmat_graph(*args, _mix(seed, salt), name=name, source=source)
     _GRAPH_CACHE[key] = g
     return g
 
 
-def workload(name, seed=0, count=None):
-    """The named workload: graph plus its query set (count overrides the size)."""
-    if name == "small_er":
-        g = graph_for("small_er", seed)
-        qs = query_set(g, count or 10, _mix(seed, 11), ("fixed", 6, 6), "induced")
-    elif name == "rmat20":
-        g = graph_for("rmat20", seed)
-        qs = query_set(g, count or 100, _mix(seed, 12), ("fixed", 12, 12), "induced",
-                       min_avg_degree=2.5)
-    elif name == "rmat20_mix":
-        g = graph_for("rmat20", seed)
-        qs = query_set(g, count or 1000, _mix(seed, 13), ("uniform", 4, 32), "tree_dense", 0.3)
-    elif name == "rmat20_train":
-        g = graph_for("rmat20", seed)
-        qs = query_set(g, count or 5000, _mix(seed, 14), ("uniform", 4, 32), "tree_dense", 0.3)
-    elif name == "rmat22":
-        g = graph_for("rmat22", seed)
-        qs = query_set(g, count or 4096, _mix(seed, 15), ("uniform", 4, 64), "tree_dense", 0.3)
-    elif name == "rmat24":
-        g = graph_for("rmat24", seed)
-        qs = query_set(g, count or 2000, _mix(seed, 16), ("geometric", 4, 99), "tree_dense", 0.3,
-                       mean=16)
-    else:
+def workload(name, seed=0, count=None, source=None, first=0):
+    """The named workload: graph plus its query set (count overrides the
+    size; first > 0 draws only queries first .. first+count-1 of the set,
+    the same queries the full set holds at those positions)."""
+    if name not in _QUERIES:
         raise ValueError(name)
+    gname, default, salt, sizes, mix, p_extra, min_deg, mean = _QUERIES[name]
+    g = graph_for(gname, seed, source)
+    total = first + (count or default)
+    qs = query_set(g, total, _mix(seed, salt), sizes, mix, p_extra, min_deg, mean, source, first=first)
     return Workload(name, g, qs)
 
 
 def write_text(path, graphs, append=False, terminate=True, first_id=0):
-    """Write graphs in the reference's text format (io/IO.cpp:87-142):
+    """Write graphs in the reference's text format (io/IO.cpp:46-128):
     't # id', a count line 'n m vertex_labels edge_labels', 'v i label' per
     vertex, 'e from to 1' per edge; the file ends with 't # -1' (without it
     the reference's reader loops at end of file). Each undirected edge is

@@ -7,9 +7,9 @@
  * Conventions shared with the reference's file format and classes:
  *   - vertex ids are 0-based, labels are 1-based unsigned (README.md);
  *   - a data graph is an undirected CSR: offsets[n+1], cols[offsets[n]] with
- *     every adjacency list sorted ascending (graph/Graph.cpp:190-226);
+ *     every adjacency list sorted ascending (graph/Graph.cpp:30-65);
  *   - a query is (qn labels, qm edges as (from, to) pairs in file order),
- *     exactly what io/IO.cpp:87-142 reads from `v`/`e` lines.
+ *     exactly what io/IO.cpp:46-128 reads from `v`/`e` lines.
  * Embeddings are non-induced, injective, undirected and edge-unlabelled.
  */
 #ifndef GPSM_H
@@ -45,7 +45,7 @@ int gpsm_gen_rmat(int scale, uint64_t m, double a, double b, double c, uint64_t 
 int gpsm_gen_labels(uint32_t n, uint32_t num_labels, double zipf_s, uint64_t seed,
                     uint32_t* labels);
 /* Undirected CSR from m undirected edges; each list sorted ascending.
- * offsets: n+1, cols: 2*m. Replaces Graph::transformToCSR (graph/Graph.cpp:190-226). */
+ * offsets: n+1, cols: 2*m. Replaces Graph::transformToCSR (graph/Graph.cpp:30-65). */
 int gpsm_csr_from_edges(uint32_t n, uint64_t m, const uint32_t* edges, uint32_t* offsets,
                         uint32_t* cols);
 /* Random-walk query of qn vertices (mode 0 induced, 1 tree, 2 dense with
@@ -57,7 +57,7 @@ int64_t gpsm_gen_query(uint32_t n, const uint32_t* offsets, const uint32_t* cols
                        uint32_t* q_edges, uint32_t* q_data_ids);
 
 /* ---- the reference's graph text format at full speed ------------------- */
-/* io/IO.cpp:87-142 reads `t # id`, a counts line, `v id label`, `e from to
+/* io/IO.cpp:46-128 reads `t # id`, a counts line, `v id label`, `e from to
  * label`, ending with `t # -1`, one fscanf per token. These parse a whole
  * file from a memory map with one thread per chunk of lines; vertices are
  * numbered in file order (the `v` id is ignored, as Graph::addVertex does).
@@ -102,7 +102,7 @@ int gpsm_graph_upload(const uint32_t* offsets, const uint32_t* cols, const uint3
 int gpsm_graph_free(gpsm_graph_t g);
 /* Builds the undirected CSR on the device from m undirected edges (pairs,
  * each edge once) and labels[n]: Graph::transformToCSR's job
- * (graph/Graph.cpp:190-226) done by a device radix sort. Same arrays as
+ * (graph/Graph.cpp:30-65) done by a device radix sort. Same arrays as
  * gpsm_csr_from_edges + gpsm_graph_upload. Scratch: the default engine. */
 int gpsm_graph_build(const uint32_t* edges, uint64_t m, const uint32_t* labels, uint32_t n,
                      gpsm_graph_t* out);
@@ -111,7 +111,7 @@ int gpsm_graph_download(gpsm_graph_t g, uint32_t* offsets, uint32_t* cols);
 int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_degree);
 /* Attaches the data graph's directed, edge-labelled edges (m pairs (from, to)
  * as in the file, labels[m] or NULL = 1) for GPSM_F_DIRECTED. The reference
- * keeps them in Graph::vertices[].out (graph/Graph.cpp:180-185). */
+ * keeps them in Graph::vertices[].out (graph/Graph.cpp:20-24). */
 int gpsm_graph_set_directed(gpsm_graph_t g, uint64_t m, const uint32_t* edges, const uint32_t* labels);
 
 #define GPSM_ORDER_PLAIN 0 /* the reference's join order (match/Match.cu:1599-1694) */
@@ -124,7 +124,7 @@ typedef struct gpsm_model_s* gpsm_model_t; /* learned join-order model (MLP on o
 #define GPSM_F_KEEP_ON_DEVICE 2u  /* rows stay in device memory; never spill to host */
 #define GPSM_F_DIRECTED 4u        /* keep rows whose query edges a->b (label) are data edges
                                      row[a]->row[b] with that label: IO::verify on the device
-                                     (io/IO.cpp:187-222); needs gpsm_graph_set_directed */
+                                     (io/IO.cpp:146-180); needs gpsm_graph_set_directed */
 
 typedef struct gpsm_match_opts {
   uint64_t cap;          /* embedding cap: stop after the first `cap` rows; 0 = none */
@@ -222,9 +222,10 @@ int gpsm_select_vertices(gpsm_engine_t e, const uint32_t* d_labels, const uint32
  * the reference. It allocates nothing: its scratch is a fixed array of about
  * 513 KiB compiled into the library (held on every GPU that loads it), so n
  * is limited to 4194304 vertices (larger n: GPSM_ERR_BUDGET). Runs on
- * `stream` (a cudaStream_t, NULL = default stream) of the current device and
- * returns after it finishes. The first call on a device looks up the array's
- * device address; make it before any stream capture. All calls share the
+ * `stream` (a cudaStream_t, NULL = default stream) of the current device;
+ * every call copies the error flags back and synchronises `stream` before it
+ * returns. The first call on a device looks up the array's device address;
+ * make it before any stream capture. All calls share the
  * array: calls that overlap on the GPU race. Needs no gpsm_init. */
 int gpsm_select_vertices_static(const uint32_t* d_labels, const uint32_t* d_offsets, uint32_t n,
                                 uint32_t label, uint32_t min_degree, uint32_t* d_out,

@@ -47,9 +47,9 @@ class Graph {
   Graph& operator=(const Graph&) = delete;
 
   // in- and out-lists merged into one undirected CSR, every list sorted
-  // ascending; label -> count lists (graph/Graph.cpp:190-265)
+  // ascending; label -> count lists (graph/Graph.cpp:30-104)
   void transformToCSR();
-  // directed, edge-labelled test used by IO::verify (graph/Graph.cpp:267-279)
+  // directed, edge-labelled test used by IO::verify (graph/Graph.cpp:107-118)
   bool isEdgeContained(VID from, VID to, LABEL label);
   void printGraph();
 

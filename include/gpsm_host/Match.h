@@ -7,7 +7,8 @@
 //   delete[] final_result;                   // caller frees, as in run.cpp
 //
 // Unlike the reference, the data graph is uploaded once per Graph object
-// (first match against it) and reused by later queries, rows are injective
+// (first match against it) and reused by later queries until that Graph is
+// deleted or its CSR rebuilt (both drop the device copy), rows are injective
 // embeddings (no homomorphism rows), and CUDA errors are reported on stderr
 // with an empty result instead of exit(1). `id_map` stays owned by Match.
 #pragma once
@@ -24,7 +25,7 @@ class Match {
   static void initGPU(int dev);
   // embedding cap for later calls (0 = none); not in the reference
   static void setCap(uint64_t cap);
-  // drops the device copy of a data graph (e.g. before deleting it)
+  // drops the device copy of a data graph now (deleting the Graph does too)
   static void releaseGraph(Graph* data);
 
  private:

@@ -20,6 +20,7 @@ REF_DISCONNECTED, REF_NO_EDGES, REF_EMPTY_CEDGE = 4, 5, 6
 vp, u32, u64, i32, i64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
 _SIG = {
     "oracle_enumerate": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, u64, vp, u64]),
+    "oracle_enumerate_ordered": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, vp]),
     "oracle_ref_plan": (vp, [u32, vp, vp, vp, u32, vp, u32, vp, vp]),
     "oracle_ref_free": (None, [vp]),
     "oracle_ref_info": (None, [vp, vp, vp, vp, vp]),
@@ -60,6 +61,86 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(vp)
 
 
+class Graph:
+    """Undirected data graph for the oracle: CSR with sorted lists."""
+
+    def __init__(self, n, offsets, cols, labels, edges=None):
+        self.n = int(n)
+        self.offsets = offsets
+        self.cols = cols
+        self.labels = labels
+        self.edges = edges
+
+
+class Query:
+    """Query graph: labels [qn] and (from, to) edges [qm, 2] in file order."""
+
+    def __init__(self, labels, edges):
+        self.labels = np.ascontiguousarray(labels, dtype=np.uint32)
+        self.edges = np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2)
+
+    @property
+    def n(self):
+        return int(self.labels.shape[0])
+
+    @property
+    def m(self):
+        return int(self.edges.shape[0])
+
+
+def csr_from_edges(n, edges):
+    """The undirected CSR of graph/Graph.cpp:30-65 built with numpy, written
+    apart from the engine's own CSR code: both directions of every edge,
+    each list sorted ascending, parallel edges kept."""
+    e = np.asarray(edges, dtype=np.uint64).reshape(-1, 2)
+    src = np.concatenate([e[:, 0], e[:, 1]])
+    dst = np.concatenate([e[:, 1], e[:, 0]])
+    key = np.sort((src << np.uint64(32)) | dst)
+    cols = (key & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    deg = np.bincount((key >> np.uint64(32)).astype(np.int64), minlength=n)
+    offsets = np.zeros(n + 1, np.uint32)
+    np.cumsum(deg, out=offsets[1:])
+    return offsets, cols
+
+
+def graph_from_edges(n, edges, labels):
+    off, cols = csr_from_edges(n, edges)
+    return Graph(n, off, cols, np.ascontiguousarray(labels, dtype=np.uint32),
+                 np.ascontiguousarray(edges, dtype=np.uint32).reshape(-1, 2))
+
+
+_GEN_SIG = {
+    "gpsm_gen_er": (C.c_int, [u32, u64, u64, vp]),
+    "gpsm_gen_rmat": (C.c_int, [C.c_int, u64, C.c_double, C.c_double, C.c_double, u64, vp]),
+    "gpsm_gen_labels": (C.c_int, [u32, u32, C.c_double, u64, vp]),
+    "gpsm_gen_query": (i64, [u32, vp, vp, vp, u32, C.c_int, C.c_double, C.c_double, u64, vp, vp, vp]),
+}
+
+
+class _GenSource:
+    """Workload source for gpsm_b200.workloads that never loads libgpsm.so:
+    the seeded generators compiled into liboracle.so and the oracle's own
+    CSR construction (csr_from_edges)."""
+
+    name = "oracle"
+
+    def lib(self):
+        lib = load()
+        if not getattr(lib, "_gen_declared", False):
+            for k, (r, a) in _GEN_SIG.items():
+                f = getattr(lib, k)
+                f.restype = r
+                f.argtypes = a
+            lib._gen_declared = True
+        return lib
+
+    def csr(self, n, edges):
+        return csr_from_edges(n, edges)
+
+
+GEN_SOURCE = _GenSource()
+
+
 def _u32(x):
     return np.ascontiguousarray(x, dtype=np.uint32)
 
@@ -80,6 +161,35 @@ def enumerate_embeddings(g, q, cap=1 << 62, rows=True, out_cap=None):
     cnt = lib.oracle_enumerate(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
                                q.m, _p(qe), cap, None, 0)
     return None, cnt
+
+
+class WorkBoundHit(Exception):
+    """The oracle's search visited its work bound before finishing."""
+
+
+def enumerate_ordered(g, q, pos2id, cap=1 << 62, work_cap=0, rows=True):
+    """The first `cap` embeddings in the lexicographic order of their values
+    taken in the vertex order pos2id (the order a join in that vertex order
+    emits them), by backtracking from the definition. Returns (rows, count):
+    rows (count, qn) with column p = query vertex pos2id[p]. Raises
+    WorkBoundHit when work_cap search nodes were visited first."""
+    lib = load()
+    qe = _u32(q.edges).reshape(-1)
+    order = np.ascontiguousarray(pos2id, dtype=np.int32)
+    out_cap = min(cap, 1 << 26) if rows else 0
+    out = np.zeros((max(out_cap, 1), q.n), np.uint32) if rows else None
+    partial = u64(0)
+    cnt = lib.oracle_enumerate_ordered(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
+                                       q.m, _p(qe), _p(order), cap, _p(out), out_cap, work_cap, C.byref(partial))
+    if cnt == -2:
+        raise ValueError("pos2id is not a permutation of the query vertices")
+    if cnt == -1:
+        raise WorkBoundHit(f"work bound {work_cap} hit after {partial.value} rows")
+    if not rows:
+        return None, cnt
+    if cnt > out_cap:
+        raise ValueError("more rows than the output holds")
+    return out[:cnt], cnt
 
 
 class RefPlan:

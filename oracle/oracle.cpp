@@ -18,7 +18,7 @@
 //      refinement ........... match/Match.cu:761-890  (4 rounds + 1 check)
 //      candidate edges ...... match/Match.cu:892-1139 (count/examine)
 //      join order + joins ... match/Match.cu:1141-1708 (table/join/expand/link)
-//      host verify .......... io/IO.cpp:187-222        (IO::verify)
+//      host verify .......... io/IO.cpp:146-180        (IO::verify)
 //    The reference's expand step may pick an edge with neither endpoint
 //    visited (match/Match.cu:1639-1650, then vpos = -1 at :1680); the
 //    restatement reports that as a defect instead of reading out of bounds.
@@ -84,7 +84,19 @@ struct Enumerator {
     return c;
   }
 
+  // A given matching order (a connected permutation): rows then come out in
+  // lexicographic order of their values taken in that order, the order in
+  // which the engine emits a join in that vertex order.
+  std::vector<uint32_t> given;
+  uint64_t work = 0, work_cap = ~0ULL;  // nodes visited; optional bound
+  bool out_by_pos = false;              // write rows in order position, not by query vertex
+
   void make_order() {
+    if (!given.empty()) {
+      order = given;
+      set_back();
+      return;
+    }
     std::vector<uint64_t> cnt(qn);
     for (uint32_t u = 0; u < qn; ++u) cnt[u] = label_count(u);
     std::vector<uint8_t> in(qn, 0);
@@ -106,6 +118,10 @@ struct Enumerator {
       order.push_back(u);
       for (uint32_t w : qadj[u]) conn[w]++;
     }
+    set_back();
+  }
+
+  void set_back() {
     back.assign(qn, {});
     std::vector<uint8_t> placed(qn, 0);
     for (uint32_t i = 0; i < qn; ++i) {
@@ -127,13 +143,17 @@ struct Enumerator {
   void emit() {
     if (out != nullptr && count < out_cap) {
       uint32_t* r = out + count * qn;
-      for (uint32_t u = 0; u < qn; ++u) r[u] = f[u];
+      for (uint32_t u = 0; u < qn; ++u) r[u] = out_by_pos ? f[order[u]] : f[u];
     }
     ++count;
   }
 
   void dfs(uint32_t pos) {
     if (count >= cap) return;
+    if (++work > work_cap) {
+      cap = count;  // stop everywhere; the caller sees the bound was hit
+      return;
+    }
     if (pos == qn) {
       emit();
       return;
@@ -209,7 +229,7 @@ struct RefQuery {
     out.assign(qn, {});
     for (uint32_t i = 0; i < qm; ++i) {
       uint32_t a = qe[2 * i], b = qe[2 * i + 1];
-      out[a].push_back(b);  // graph/Graph.cpp:180-185
+      out[a].push_back(b);  // graph/Graph.cpp:20-24
       in[b].push_back(a);
       qm_from.push_back(a);
       qm_to.push_back(b);
@@ -273,7 +293,7 @@ static void ref_edges(RefPlan& P) {
 
 static void ref_spanning_order(const DataGraph& g, RefPlan& P) {
   const RefQuery& q = P.q;
-  // label frequencies of the data graph (Graph::inverse_num, graph/Graph.cpp:228-262)
+  // label frequencies of the data graph (Graph::inverse_num, graph/Graph.cpp:66-102)
   std::vector<float> score(q.n);
   for (uint32_t i = 0; i < q.n; ++i) {
     float num = 0.0f;
@@ -626,6 +646,35 @@ int64_t oracle_enumerate(uint32_t n, const uint32_t* off, const uint32_t* col, c
   return (int64_t)en.count;
 }
 
+// The same backtracking in a given vertex order (pos2id: a connected
+// permutation of the query vertices). Candidates of each position are taken
+// in ascending data-vertex order, so rows are found in lexicographic order
+// of (row[pos2id[0]], row[pos2id[1]], ...): the first `cap` rows are the
+// first `cap` of that order. Rows are written in position order (column p =
+// query vertex pos2id[p]), unsorted. Returns the count (at most cap), or -1
+// when work_cap search nodes were visited first (0 = no bound); then
+// *partial gets the rows found so far.
+int64_t oracle_enumerate_ordered(uint32_t n, const uint32_t* off, const uint32_t* col, const uint32_t* lab,
+                                 uint32_t qn, const uint32_t* qlab, uint32_t qm, const uint32_t* qe,
+                                 const int32_t* pos2id, uint64_t cap, uint32_t* out, uint64_t out_cap,
+                                 uint64_t work_cap, uint64_t* partial) {
+  DataGraph g{n, off, col, lab};
+  Enumerator en(g, qn, qlab, qm, qe, cap, out, out_cap);
+  std::vector<uint8_t> seen(qn, 0);
+  for (uint32_t p = 0; p < qn; ++p) {
+    const int32_t u = pos2id[p];
+    if (u < 0 || (uint32_t)u >= qn || seen[u]) return -2;
+    seen[u] = 1;
+    en.given.push_back((uint32_t)u);
+  }
+  en.out_by_pos = true;
+  if (work_cap) en.work_cap = work_cap;
+  en.run();
+  if (partial) *partial = en.count;
+  if (en.work > en.work_cap) return -1;
+  return (int64_t)en.count;
+}
+
 // ---- restatement of the reference pipeline --------------------------------
 // Runs edge list, spanning order, init, refinement, candidate edges (both
 // directions) and the plain join order. *status gets a RefStatus.
@@ -751,7 +800,7 @@ int64_t oracle_ref_join(void* h, int injective, uint64_t cap, uint64_t* level_ro
   return (int64_t)J.final_rows;
 }
 
-// IO::verify (io/IO.cpp:187-222) for one row in table-column order: the row
+// IO::verify (io/IO.cpp:146-180) for one row in table-column order: the row
 // must be injective and every query edge (from -> to, file order) must be a
 // data edge stored as from -> to in the data file. data_from/data_to hold the
 // data file's edges sorted by (from, to).

@@ -16,7 +16,17 @@ ARCH := -gencode arch=compute_100a,code=sm_100a
 SHIM := -include ref/shim.h -Iref/stub
 OBJS := $(OUT)/Util.o $(OUT)/Graph.o $(OUT)/IO.o $(OUT)/Match.o
 
-all: $(OUT)/GpSM.exe $(OUT)/ref_driver
+all: $(OUT)/GpSM.exe $(OUT)/ref_driver $(OUT)/run_dropin
+
+# The reference's own driver main/run.cpp, unmodified, compiled against this
+# library's drop-in Graph/IO/Match (include/gpsm_host/) and linked with
+# libgpsm.so. It is fed to the compiler on standard input from
+# ref/dropin/main/, so its `#include "../io/IO.h"` lines resolve to the shim
+# headers under ref/dropin/ instead of the reference's own classes.
+LIBDIR := $(abspath ../gpsm_b200)
+$(OUT)/run_dropin: $(REF)/main/run.cpp $(wildcard ref/dropin/*/*.h) $(LIBDIR)/libgpsm.so | $(OUT)
+	cd ref/dropin/main && g++ -O2 -w -std=c++17 -I$(abspath ../include) -x c++ - -o $(abspath $@) \
+	  -L$(LIBDIR) -lgpsm -Wl,-rpath,'$$ORIGIN/../../gpsm_b200' < $(REF)/main/run.cpp
 
 $(OUT):
 	mkdir -p $(OUT)

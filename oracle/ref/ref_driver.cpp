@@ -1,7 +1,7 @@
 // ORACLE (test infrastructure): a driver linked against the reference's own
 // objects (built from the unmodified sources by oracle/ref.mk). For every
 // query it calls the reference's Match::match and dumps the raw result table
-// BEFORE IO::verify's directed/edge-label filter (io/IO.cpp:187-222), so the
+// BEFORE IO::verify's directed/edge-label filter (io/IO.cpp:146-180), so the
 // reference's undirected matches can be compared with the oracle's.
 //
 //   ref_driver DATA QUERY OUT.bin [dev]

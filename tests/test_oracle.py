@@ -16,7 +16,8 @@ from gpsm_b200 import workloads as W
 
 
 def graph(n, edges, labels):
-    return W.graph_from_edges(n, np.array(edges, np.uint32).reshape(-1, 2), np.array(labels, np.uint32))
+    # the oracle's own CSR: these tests never run the engine's code
+    return oracle.graph_from_edges(n, np.array(edges, np.uint32).reshape(-1, 2), np.array(labels, np.uint32))
 
 
 def query(labels, edges):
@@ -145,3 +146,36 @@ def test_explore_semantics_skip_after_first_failing_target(lib):
     assert np.flatnonzero(c[0]).tolist() == [3]  # A cleared
     assert np.flatnonzero(c[1]).tolist() == [4]
     assert np.flatnonzero(c[2]).tolist() == [5]  # not 1: A stopped at target 1
+
+
+def test_oracle_csr_equals_engine_csr(lib):
+    """The oracle's numpy CSR and the engine's gpsm_csr_from_edges agree,
+    parallel edges included, so a CSR bug cannot hide on both sides."""
+    rng = np.random.default_rng(3)
+    for n, m in [(1, 0), (7, 12), (500, 4000), (20_000, 150_000)]:
+        e = rng.integers(0, n, size=(m, 2)).astype(np.uint32)
+        o = oracle.csr_from_edges(n, e)
+        g = W.graph_from_edges(n, e, np.ones(n, np.uint32))
+        assert np.array_equal(o[0], g.offsets) and np.array_equal(o[1], g.cols)
+
+
+@pytest.mark.parametrize("name", ["small_er", "rmat20_mix"])
+def test_oracle_source_draws_the_engine_workloads(lib, name):
+    """Workloads drawn without libgpsm.so (what bench.py's reference arm
+    uses) are the ones the engine's source draws: same graph, CSR and
+    queries; a window [first, first+count) equals that slice of the set."""
+    if name == "rmat20_mix":  # the graph shape at a size the CPU suite affords
+        W._GRAPHS["_t14"] = ("rmat", (14, 1 << 17, 16, 1.0), 9)
+        W._QUERIES["_t14_mix"] = ("_t14", 30, 13, ("uniform", 4, 32), "tree_dense", 0.3, 0.0, None)
+        name = "_t14_mix"
+    a = W.workload(name)
+    b = W.workload(name, source=oracle.GEN_SOURCE)
+    for x, y in [(a.graph.offsets, b.graph.offsets), (a.graph.cols, b.graph.cols),
+                 (a.graph.labels, b.graph.labels), (a.graph.edges, b.graph.edges)]:
+        assert np.array_equal(x, y)
+    assert len(a.queries) == len(b.queries)
+    for qa, qb in zip(a.queries, b.queries):
+        assert np.array_equal(qa.labels, qb.labels) and np.array_equal(qa.edges, qb.edges)
+    w = W.workload(name, first=3, count=4, source=oracle.GEN_SOURCE)
+    for qa, qb in zip(a.queries[3:7], w.queries):
+        assert np.array_equal(qa.labels, qb.labels) and np.array_equal(qa.edges, qb.edges)

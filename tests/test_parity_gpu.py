@@ -239,7 +239,7 @@ def test_select_vertices_matches_label_degree_filter(gpu, lib):
 
 
 def test_directed_labelled_mode_equals_host_verify(gpu, small_er):
-    """GPSM_F_DIRECTED keeps exactly the rows io/IO.cpp:187-222 keeps: every
+    """GPSM_F_DIRECTED keeps exactly the rows io/IO.cpp:146-180 keeps: every
     query edge a -> b (label l) must be a data edge row[a] -> row[b] with l."""
     g = small_er.graph
     rng = np.random.default_rng(3)

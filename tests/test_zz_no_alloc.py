@@ -48,6 +48,28 @@ def test_static_scratch_variant_matches_allocating_entry_point(gpu, lib):
         assert np.array_equal(want.astype(np.int64), np.flatnonzero((g.labels == label) & (deg >= d)))
 
 
+def test_static_scratch_variant_at_its_limit_then_small(gpu, lib):
+    """n = 2^22 fills the whole static bitmap and uses every compaction tile;
+    a smaller graph right after must not see the larger call's bits."""
+    import torch
+    rng = np.random.default_rng(5)
+    for n in (1 << 22, 70_001):
+        labels = rng.integers(1, 9, size=n).astype(np.int32)
+        deg = rng.integers(0, 6, size=n)
+        offsets = np.concatenate([[0], np.cumsum(deg)]).astype(np.int32)
+        lab = torch.from_numpy(labels).cuda()
+        off = torch.from_numpy(offsets).cuda()
+        out_a = torch.zeros(n, dtype=torch.int32, device="cuda")
+        out_b = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cnt_a = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cnt_b = torch.zeros(1, dtype=torch.int32, device="cuda")
+        for label, d in [(2, 1), (7, 4)]:
+            want = np.flatnonzero((labels == label) & (deg >= d))
+            got = _select(lib, "static", lab, off, n, label, d, out_b, cnt_b)
+            assert np.array_equal(got.astype(np.int64), want), (n, label, d)
+            assert np.array_equal(_select(lib, "alloc", lab, off, n, label, d, out_a, cnt_a), got)
+
+
 def test_static_scratch_variant_rejects_graphs_over_its_limit(gpu, lib):
     import torch
     lab = torch.zeros(1, dtype=torch.int32, device="cuda")

@@ -241,16 +241,21 @@ def pack_queries(queries):
 
 
 def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None, level_bytes=0, slots=1,
-                model=None, slot_arena=0):
+                model=None, slot_arena=0, work_cap=0):
     """Match queries back to back (rows stay on the device); slots > 1 runs
     them on that many engine slots at once (continuous batching); orders:
-    None (plain), "learned" (model) or a list of pos2id per query.
-    Returns (counts, capped, per-query device ms, batch info dict)."""
+    None (plain), "learned" (model) or a list of pos2id per query; work_cap:
+    candidates a query's joins may scan (0 = no bound).
+    Returns (counts, capped, per-query device ms, batch info dict): capped
+    is True where the embedding cap or the work cap stopped a query; the
+    info dict's "aborted" counts the work-cap stops and "stop" holds the
+    per-query codes (0 complete, 1 embedding cap, 2 work cap)."""
     lib = _lib.load()
     voff, ql, eoff, qe = packed if packed is not None else pack_queries(queries)
     nq = len(voff) - 1
     opts = _lib.MatchOpts()
     opts.cap = int(cap or 0)
+    opts.work_cap = int(work_cap)
     opts.level_bytes = int(level_bytes)
     ords = None
     if isinstance(orders, str) and orders == "learned":
@@ -274,6 +279,8 @@ def match_batch(dgraph, queries, cap=None, orders=None, engine=None, packed=None
                                   C.byref(info))
     _lib.check(rc, "gpsm_match_batch")
     d = {k: getattr(info, k) for k, _ in _lib.BatchInfo._fields_}
+    d["aborted"] = int((capped == 2).sum())
+    d["stop"] = capped.copy()
     return counts, capped.astype(bool), qms, d
 
 

@@ -68,6 +68,7 @@ SIGNATURES = {
     "gpsm_debug_filter": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_match_batch": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_flush_l2": (C.c_int, [vp, u64]),
+    "gpsm_debug_skew_scan_tickets": (C.c_int, [vp, u32]),
     "gpsm_select_vertices": (C.c_int, [vp, vp, vp, u32, u32, u32, vp, vp]),
     "gpsm_select_vertices_static": (C.c_int, [vp, vp, u32, u32, u32, vp, vp, vp]),
     "gpsm_last_levels": (C.c_int, [vp, u32, vp, vp, vp]),
@@ -111,7 +112,7 @@ class MatchInfo(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", u32), ("ext_blocks_per_sm", u32), ("step_cands", u64), ("level_bytes", u64),
-                ("slots", u32), ("pad", u32), ("race_share", u64)]
+                ("slots", u32), ("scan_spin_limit", u32), ("race_share", u64)]
 
 
 class RequestInfo(C.Structure):

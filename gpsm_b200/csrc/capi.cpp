@@ -349,6 +349,7 @@ int gpsm_set_tuning(const gpsm_tuning* t) {
   if (t->level_bytes) T.level_bytes = std::max<uint64_t>(t->level_bytes, 1u << 20);
   if (t->slots) T.slots = std::min<uint32_t>(t->slots, 64);
   if (t->race_share) T.race_share = t->race_share;
+  if (t->scan_spin_limit) T.scan_spin_limit = t->scan_spin_limit;
   return GPSM_OK;
 }
 
@@ -360,7 +361,7 @@ int gpsm_get_tuning(gpsm_tuning* t) {
   t->step_cands = T.step_cands;
   t->level_bytes = T.level_bytes;
   t->slots = T.slots;
-  t->pad = 0;
+  t->scan_spin_limit = T.scan_spin_limit;
   t->race_share = T.race_share;
   return GPSM_OK;
 }
@@ -573,6 +574,21 @@ int gpsm_flush_l2(gpsm_engine_t eng, uint64_t bytes) {
     bytes = std::min<uint64_t>(bytes, ws.arena.size);
     GPSM_CUDA(cudaMemsetAsync(ws.arena.base, 0x5a, bytes, ws.stream));
     GPSM_CUDA(cudaStreamSynchronize(ws.stream));
+    return GPSM_OK;
+  });
+}
+
+int gpsm_debug_skew_scan_tickets(gpsm_engine_t eng, uint32_t k) {
+  gpsm_engine_s* e = engine_or_default(eng);
+  if (!e) return GPSM_ERR_STATE;
+  return guarded([&]() -> int {
+    std::lock_guard<std::mutex> lk(e->mu);
+    Workspace& ws = *e->ws;
+    unsigned long long c = 0;
+    GPSM_CUDA(cudaStreamSynchronize(ws.stream));
+    GPSM_CUDA(cudaMemcpy(&c, ws.scan.d_ticket, sizeof(c), cudaMemcpyDeviceToHost));
+    c += k;
+    GPSM_CUDA(cudaMemcpy(ws.scan.d_ticket, &c, sizeof(c), cudaMemcpyHostToDevice));
     return GPSM_OK;
   });
 }

@@ -548,6 +548,7 @@ static Lookback make_lb(Workspace& ws, uint32_t tiles) {
   lb.base = base;
   lb.epoch = ep;
   lb.flags = ws.d_flags;
+  lb.spin_limit = tuning().scan_spin_limit;
   return lb;
 }
 

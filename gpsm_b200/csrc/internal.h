@@ -109,6 +109,9 @@ struct Tuning {
   // order: about 20 ms of joins on one B200, enough for a capped query of
   // 10^7 embeddings in a good order
   uint64_t race_share = 1ull << 28;
+  // polls of one predecessor's status a look-back makes before giving up
+  // (DF_SCAN_TIMEOUT): the bound on every inter-block wait
+  uint32_t scan_spin_limit = 1u << 22;
 };
 Tuning& tuning();
 int sm_count();

@@ -448,6 +448,7 @@ static Lookback next_lb(Workspace& ws, uint64_t tiles) {
   lb.base = base;
   lb.epoch = ep;
   lb.flags = ws.d_flags;
+  lb.spin_limit = tuning().scan_spin_limit;
   return lb;
 }
 

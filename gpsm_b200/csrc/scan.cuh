@@ -25,11 +25,11 @@ struct Lookback {
   unsigned long long base;
   uint32_t epoch;
   uint32_t* flags;
+  uint32_t spin_limit;  // polls of one predecessor before giving up (tuning().scan_spin_limit)
 };
 
 constexpr int kLbValueBits = 42;
 constexpr unsigned long long kLbValueMask = (1ULL << kLbValueBits) - 1;
-constexpr unsigned kLbSpinLimit = 1u << 22;
 
 __device__ __forceinline__ unsigned long long lb_word(uint32_t epoch, uint32_t flag,
                                                       unsigned long long v) {
@@ -75,7 +75,7 @@ __device__ __forceinline__ unsigned long long lb_exclusive(const Lookback& lb, u
         ep = (uint32_t)(w >> 44);
         flag = (uint32_t)((w >> 42) & 3);
         if (ep == lb.epoch && flag != 0) break;
-        if (++spins > kLbSpinLimit) {
+        if (++spins > lb.spin_limit) {
           timed_out = true;
           flag = 2;
           break;

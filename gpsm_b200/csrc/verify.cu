@@ -90,6 +90,7 @@ void launch_verify_directed(Workspace& ws, const uint32_t* in, uint64_t nrows, u
   lb.base = base;
   lb.epoch = ep;
   lb.flags = ws.d_flags;
+  lb.spin_limit = tuning().scan_spin_limit;
   k_verify_directed<<<(uint32_t)tiles, kVerBlock, 0, ws.stream>>>(in, nrows, cols, d_checks, nchecks, off, col, lab,
                                                                    out, d_kept, lb);
   GPSM_LAUNCHED();

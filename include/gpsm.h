@@ -268,6 +268,14 @@ int gpsm_server_destroy(gpsm_server_t s);
 
 /* Writes `bytes` of device memory on the engine's stream (an L2 flush). */
 int gpsm_flush_l2(gpsm_engine_t e, uint64_t bytes);
+/* Testing aid for the bounded device waits (no counterpart in the
+ * reference): takes k stray tickets from the engine's look-back ticket
+ * counter without telling the host, so the next query's scans wait on
+ * predecessor tiles that never publish. Those waits give up after
+ * scan_spin_limit polls (gpsm_set_tuning) and that query returns
+ * GPSM_ERR_TIMEOUT; the engine re-reads the counter before its next query,
+ * which then runs normally. */
+int gpsm_debug_skew_scan_tickets(gpsm_engine_t e, uint32_t k);
 
 /* Per-width join statistics of the engine's last gpsm_match_ex/
  * gpsm_engine_match call (n+1 entries each, index = table width):
@@ -285,7 +293,9 @@ typedef struct gpsm_tuning {
   uint64_t step_cands;         /* candidates one join step may admit (default 2^25) */
   uint64_t level_bytes;        /* bytes per intermediate join level (default 256 MiB) */
   uint32_t slots;              /* engine slots for batches and serving (default 4) */
-  uint32_t pad;
+  uint32_t scan_spin_limit;    /* polls a look-back scan makes of one predecessor before it gives up,
+                                  flags the launch and the call returns GPSM_ERR_TIMEOUT
+                                  (default 2^22; ~a second at most) */
   uint64_t race_share;         /* learned order: first work share (candidates) when the learned plan
                                   and the plain order take turns (default 2^28) */
 } gpsm_tuning;

@@ -20,7 +20,7 @@ REF_DISCONNECTED, REF_NO_EDGES, REF_EMPTY_CEDGE = 4, 5, 6
 vp, u32, u64, i32, i64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
 _SIG = {
     "oracle_enumerate": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, u64, vp, u64]),
-    "oracle_enumerate_ordered": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, vp]),
+    "oracle_enumerate_ordered": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, vp, vp]),
     "oracle_ref_plan": (vp, [u32, vp, vp, vp, u32, vp, u32, vp, vp]),
     "oracle_ref_free": (None, [vp]),
     "oracle_ref_info": (None, [vp, vp, vp, vp, vp]),
@@ -167,29 +167,59 @@ class WorkBoundHit(Exception):
     """The oracle's search visited its work bound before finishing."""
 
 
-def enumerate_ordered(g, q, pos2id, cap=1 << 62, work_cap=0, rows=True):
+def enumerate_ordered(g, q, pos2id, cap=1 << 62, work_cap=0, rows=True, with_digest=False):
     """The first `cap` embeddings in the lexicographic order of their values
     taken in the vertex order pos2id (the order a join in that vertex order
-    emits them), by backtracking from the definition. Returns (rows, count):
-    rows (count, qn) with column p = query vertex pos2id[p]. Raises
-    WorkBoundHit when work_cap search nodes were visited first."""
+    emits them), by backtracking from the definition. Returns (rows, count)
+    or, with_digest, (rows, count, digest): rows (count, qn) with column p =
+    query vertex pos2id[p] (None when rows=False); digest = rows_digest of
+    all `count` rows, computed while searching. Raises WorkBoundHit when
+    work_cap search steps (nodes and candidates examined) came first."""
     lib = load()
     qe = _u32(q.edges).reshape(-1)
     order = np.ascontiguousarray(pos2id, dtype=np.int32)
     out_cap = min(cap, 1 << 26) if rows else 0
     out = np.zeros((max(out_cap, 1), q.n), np.uint32) if rows else None
     partial = u64(0)
+    dig = u64(0)
     cnt = lib.oracle_enumerate_ordered(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
-                                       q.m, _p(qe), _p(order), cap, _p(out), out_cap, work_cap, C.byref(partial))
+                                       q.m, _p(qe), _p(order), cap, _p(out), out_cap, work_cap, C.byref(partial),
+                                       C.byref(dig))
     if cnt == -2:
         raise ValueError("pos2id is not a permutation of the query vertices")
     if cnt == -1:
         raise WorkBoundHit(f"work bound {work_cap} hit after {partial.value} rows")
-    if not rows:
-        return None, cnt
-    if cnt > out_cap:
+    if rows and cnt > out_cap:
         raise ValueError("more rows than the output holds")
-    return out[:cnt], cnt
+    r = out[:cnt] if rows else None
+    return (r, cnt, dig.value) if with_digest else (r, cnt)
+
+
+_M1, _M2 = np.uint64(0xBF58476D1CE4E5B9), np.uint64(0x94D049BB133111EB)
+
+
+def _fold(z):
+    z = (z ^ (z >> np.uint64(30))) * _M1
+    z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def rows_digest(rows, chunk=1 << 22):
+    """Order-sensitive digest of a table (rows in order, columns in position
+    order): sum over rows i of (i + 1) * hash(row i) mod 2^64, the hash a
+    splitmix64-style fold of (value | position << 32). Same value as the
+    digest enumerate_ordered computes while searching."""
+    rows = np.asarray(rows)
+    total = np.uint64(0)
+    with np.errstate(over="ignore"):
+        for a in range(0, rows.shape[0], chunk):
+            blk = rows[a:a + chunk]
+            h = np.full(blk.shape[0], 0x243F6A8885A308D3, np.uint64)
+            for p in range(blk.shape[1]):
+                h = _fold(h ^ (blk[:, p].astype(np.uint64) | (np.uint64(p) << np.uint64(32))))
+            w = np.arange(a + 1, a + 1 + blk.shape[0], dtype=np.uint64)
+            total = total + np.sum(h * w, dtype=np.uint64)
+    return int(total)
 
 
 class RefPlan:

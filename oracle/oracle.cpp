@@ -88,8 +88,9 @@ struct Enumerator {
   // lexicographic order of their values taken in that order, the order in
   // which the engine emits a join in that vertex order.
   std::vector<uint32_t> given;
-  uint64_t work = 0, work_cap = ~0ULL;  // nodes visited; optional bound
+  uint64_t work = 0, work_cap = ~0ULL;  // nodes and candidates visited; optional bound
   bool out_by_pos = false;              // write rows in order position, not by query vertex
+  uint64_t digest = 0;                  // rows_digest of the rows found, in order (by position)
 
   void make_order() {
     if (!given.empty()) {
@@ -145,7 +146,21 @@ struct Enumerator {
       uint32_t* r = out + count * qn;
       for (uint32_t u = 0; u < qn; ++u) r[u] = out_by_pos ? f[order[u]] : f[u];
     }
+    if (out_by_pos) digest += row_hash(f, order) * (count + 1);
     ++count;
+  }
+
+  // Hash of one row, values taken in position order: a splitmix64-style
+  // fold of (value | position << 32); oracle.rows_digest restates it in numpy.
+  static uint64_t fold(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  }
+  static uint64_t row_hash(const std::vector<uint32_t>& f, const std::vector<uint32_t>& order) {
+    uint64_t h = 0x243f6a8885a308d3ULL;
+    for (uint32_t p = 0; p < order.size(); ++p) h = fold(h ^ ((uint64_t)f[order[p]] | ((uint64_t)p << 32)));
+    return h;
   }
 
   void dfs(uint32_t pos) {
@@ -161,6 +176,10 @@ struct Enumerator {
     uint32_t u = order[pos];
     if (back[pos].empty()) {
       for (uint32_t y = 0; y < g.n && count < cap; ++y) {
+        if (++work > work_cap) {  // every candidate examined counts
+          cap = count;
+          return;
+        }
         if (!fits(pos, y)) continue;
         f[u] = y;
         used[y] = 1;
@@ -177,6 +196,10 @@ struct Enumerator {
     const uint32_t* e = g.col + g.off[f[p] + 1];
     uint32_t prev = 0xffffffffu;
     for (; a < e && count < cap; ++a) {
+      if (++work > work_cap) {
+        cap = count;
+        return;
+      }
       uint32_t y = *a;
       if (y == prev) continue;  // parallel data edges give one embedding
       prev = y;
@@ -651,13 +674,15 @@ int64_t oracle_enumerate(uint32_t n, const uint32_t* off, const uint32_t* col, c
 // in ascending data-vertex order, so rows are found in lexicographic order
 // of (row[pos2id[0]], row[pos2id[1]], ...): the first `cap` rows are the
 // first `cap` of that order. Rows are written in position order (column p =
-// query vertex pos2id[p]), unsorted. Returns the count (at most cap), or -1
-// when work_cap search nodes were visited first (0 = no bound); then
+// query vertex pos2id[p]), unsorted, up to out_cap of them; *digest gets an
+// order-sensitive digest of all `count` rows (sum over rows i of
+// (i + 1) * hash(row i), mod 2^64). Returns the count (at most cap), or -1
+// when work_cap search steps (nodes and candidates examined) came first (0 = no bound); then
 // *partial gets the rows found so far.
 int64_t oracle_enumerate_ordered(uint32_t n, const uint32_t* off, const uint32_t* col, const uint32_t* lab,
                                  uint32_t qn, const uint32_t* qlab, uint32_t qm, const uint32_t* qe,
                                  const int32_t* pos2id, uint64_t cap, uint32_t* out, uint64_t out_cap,
-                                 uint64_t work_cap, uint64_t* partial) {
+                                 uint64_t work_cap, uint64_t* partial, uint64_t* digest) {
   DataGraph g{n, off, col, lab};
   Enumerator en(g, qn, qlab, qm, qe, cap, out, out_cap);
   std::vector<uint8_t> seen(qn, 0);
@@ -671,6 +696,7 @@ int64_t oracle_enumerate_ordered(uint32_t n, const uint32_t* off, const uint32_t
   if (work_cap) en.work_cap = work_cap;
   en.run();
   if (partial) *partial = en.count;
+  if (digest) *digest = en.digest;
   if (en.work > en.work_cap) return -1;
   return (int64_t)en.count;
 }
@@ -871,23 +897,25 @@ double oracle_cpu_pipeline(uint32_t n, const uint32_t* off, const uint32_t* col,
   if (threads < 1) threads = 1;
   std::vector<std::thread> ts;
   for (int t = 0; t < threads; ++t) ts.emplace_back(work);
-  if (deadline_s > 0) {
-    // watchdog: raise the abort flag at the deadline
-    std::thread([&] {
-      while (!abort_flag.load()) {
+  // watchdog: raises the abort flag at the deadline; joined before return
+  // (it reads this frame's locals)
+  std::atomic<int> workers_done(0);
+  std::thread watchdog;
+  if (deadline_s > 0)
+    watchdog = std::thread([&] {
+      while (!workers_done.load()) {
         double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el >= deadline_s) {
           abort_flag.store(1);
           break;
         }
-        if (next.load() >= nq + (uint32_t)threads) break;
         std::this_thread::sleep_for(std::chrono::milliseconds(20));
       }
-    }).detach();
-  }
+    });
   for (auto& th : ts) th.join();
   double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  abort_flag.store(1);
+  workers_done.store(1);
+  if (watchdog.joinable()) watchdog.join();
   return el;
 }
 

@@ -18,17 +18,19 @@ def _rank(rank, world, port, q):
                       LOCAL_RANK=str(rank))
     sys.path.insert(0, ROOT)
     import bench
-    r, w, local, pg = bench.dist_setup(world)
+    r, w, local, pg = bench.dist_setup()
     assert (r, w) == (rank, world) and pg is not None
-    wl = bench.load_workload("small_er", rank)
+    bounds = bench.slice_bounds(4096, 20)
+    mine = [bench.slice_of(k, rank, world, len(bounds)) for k in range(10)]
+    sizes = [bounds[s][1] - bounds[s][0] for s in mine]
     bench.barrier(pg)
     mx = bench.max_over_ranks(pg, 10.0 + rank)
-    sm = bench.sum_over_ranks(pg, len(wl.queries))
-    q.put((rank, mx, sm, [int(x) for x in wl.queries[0].labels], len(wl.queries)))
+    sm = bench.sum_over_ranks(pg, sum(sizes))
+    q.put((rank, mx, sm, mine, sizes))
     pg.destroy_process_group()
 
 
-def test_two_gloo_ranks_reduce_and_get_equal_sized_batches():
+def test_two_gloo_ranks_reduce_and_take_disjoint_equal_sized_slices():
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = 29500 + os.getpid() % 1000
@@ -40,17 +42,23 @@ def test_two_gloo_ranks_reduce_and_get_equal_sized_batches():
         assert p.exitcode == 0
     res = sorted(q.get(timeout=10) for _ in range(2))
     assert res[0][1] == res[1][1] == 11.0          # max over ranks
-    assert res[0][2] == res[1][2] == 20.0          # total work over ranks
-    assert res[0][4] == res[1][4]                  # same batch size per rank (weak scaling)
+    assert res[0][2] == res[1][2] == sum(res[0][4]) + sum(res[1][4])  # total work over ranks
+    # ten steps of two ranks cover the twenty slices once, each slice by one rank
+    assert sorted(res[0][3] + res[1][3]) == list(range(20))
+    assert all(abs(a - b) <= 1 for a, b in zip(res[0][4], res[1][4]))  # weak scaling: equal work per rank
 
 
-def test_reference_arm_prints_one_json_line():
-    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
-                          "small_er", "--steps", "1", "--warmup", "0", "--cpu-seconds", "2"],
-                         capture_output=True, text=True, timeout=300, cwd=ROOT)
+def test_reference_arm_prints_one_json_line_without_the_engine():
+    """The reference arm draws its workload through the oracle: libgpsm.so
+    is never mapped in its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'small_er', "
+            "'--steps', '1', '--warmup', '0']; runpy.run_path('bench.py', run_name='__main__'); "
+            "print('MAPPED', 'libgpsm' in open('/proc/self/maps').read())")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=ROOT)
     assert out.returncode == 0, out.stderr
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
+    assert "MAPPED False" in out.stdout

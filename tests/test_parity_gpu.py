@@ -204,14 +204,18 @@ def rmat20(gpu):
 
 
 def test_rmat20_filter_and_capped_rows(gpu, rmat20):
+    """Bench queries 0, 1, 3 and 4 of the rmat20 set (query 2's plain order
+    explores billions of dead-end rows before its first embedding, on the
+    GPU as in the restatement): filter products, then the first 50,000 rows
+    in the plain order equal the restated reference join's."""
     wl, dg = rmat20
     g = wl.graph
-    for q in wl.queries[:4]:
+    for i in (0, 1, 3, 4):
+        q = wl.queries[i]
         plan, _ = check_filter(gpu, dg, g, q)
-        ref_rows, ref_cnt, _, capped = plan.join(injective=True, cap=50000, work_cap=int(5e7))
+        ref_rows, ref_cnt, _, capped = plan.join(injective=True, cap=50000, work_cap=int(2e9))
+        assert ref_cnt == 50000, (i, ref_cnt)  # stopped by the cap, not by the work bound
         out = gpu.match(dg, q, cap=50000)
-        if capped and ref_cnt < 50000:
-            continue  # oracle stopped on its work bound, not on the cap
         assert out.count == ref_cnt
         assert np.array_equal(out.rows, ref_rows)
 

@@ -400,12 +400,14 @@ class Server:
                                           1 if collect_rows else 0, C.byref(h)), "gpsm_server_create")
         self.handle = h
         self.collect = collect_rows
+        self._qn = {}  # ticket -> query vertices, for requests not yet collected
 
     def submit(self, query):
         ql, qe = _query_arrays(query)
         t = C.c_uint64(0)
         _lib.check(self._lib.gpsm_server_submit(self.handle, query.n, _lib.ptr(ql), query.m, _lib.ptr(qe),
                                                 C.byref(t)), "gpsm_server_submit")
+        self._qn[t.value] = query.n
         return t.value, query.n
 
     def wait(self, ticket, timeout=-1.0, raise_on_error=True):
@@ -419,8 +421,29 @@ class Server:
         idm = np.zeros(qn, np.int32)
         rc = self._lib.gpsm_server_wait(self.handle, tid, float(timeout), C.byref(info),
                                         C.byref(out) if self.collect else None, _lib.ptr(idm))
+        return self._result(rc, info, out, idm, tid, qn, raise_on_error, "gpsm_server_wait")
+
+    def wait_any(self, timeout=-1.0, raise_on_error=True):
+        """(ticket, info) of the first finished request not yet collected,
+        in completion order (same info as wait())."""
+        info = _lib.RequestInfo()
+        info.status = 1
+        out = _lib.vp()
+        idm = np.zeros(128, np.int32)
+        t = C.c_uint64(0)
+        rc = self._lib.gpsm_server_wait_any(self.handle, float(timeout), C.byref(t), C.byref(info),
+                                            C.byref(out) if self.collect else None, _lib.ptr(idm))
+        if rc != 0 and info.status == 1:
+            _lib.check(rc, "gpsm_server_wait_any")
+        qn = self._qn.get(t.value, 0)
+        return (t.value, qn), self._result(rc, info, out, idm[:qn].copy(), t.value, qn, raise_on_error,
+                                           "gpsm_server_wait_any")
+
+    def _result(self, rc, info, out, idm, tid, qn, raise_on_error, what):
+        if info.status != 1:  # collected (a timeout leaves the request outstanding)
+            self._qn.pop(tid, None)
         if rc != 0 and (raise_on_error or info.status == 1):
-            _lib.check(rc, "gpsm_server_wait")
+            _lib.check(rc, what)
         if rc != 0:
             return {k: getattr(info, k) for k, _ in _lib.RequestInfo._fields_} | {
                 "error": self._lib.gpsm_last_error().decode(errors="replace")}

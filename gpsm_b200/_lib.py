@@ -76,6 +76,7 @@ SIGNATURES = {
     "gpsm_server_create": (C.c_int, [vp, u32, u64, u64, vp, i32, vp]),
     "gpsm_server_submit": (C.c_int, [vp, u32, vp, u32, vp, vp]),
     "gpsm_server_wait": (C.c_int, [vp, u64, f64, vp, vp, vp]),
+    "gpsm_server_wait_any": (C.c_int, [vp, f64, vp, vp, vp, vp]),
     "gpsm_server_stats": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "gpsm_server_destroy": (C.c_int, [vp]),
     "gpsm_set_tuning": (C.c_int, [vp]),
@@ -112,7 +113,8 @@ class MatchInfo(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", u32), ("ext_blocks_per_sm", u32), ("step_cands", u64), ("level_bytes", u64),
-                ("slots", u32), ("scan_spin_limit", u32), ("race_share", u64)]
+                ("slots", u32), ("scan_spin_limit", u32), ("race_share", u64),
+                ("ext_items", u32), ("pad", u32)]
 
 
 class RequestInfo(C.Structure):

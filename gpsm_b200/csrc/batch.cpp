@@ -13,6 +13,7 @@
 //                                request (submit, start, end).
 // The reference has neither: main/run.cpp matches one query after another
 // and re-uploads the data graph for each (match/Match.cu:1714).
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -79,6 +80,10 @@ struct BatchOut {
 
 // Runs queries [0, nq) on the pool's slots. Device time of the batch is the
 // span from the earliest slot's start event to the latest slot's end event.
+// Slots take the queries largest first (query edges, then vertices; ties in
+// batch order): a long query starts while the others still run instead of
+// running alone at the end (longest-processing-time-first dispatch).
+// Results stay indexed by the query's place in the batch.
 int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const uint32_t* q_voff,
                        const uint32_t* q_labels, const uint64_t* q_eoff, const uint32_t* q_edges,
                        const MatchOptions& base, const int32_t* orders, BatchOut& out) {
@@ -87,6 +92,13 @@ int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const 
   out.capped.assign(nq, 0);
   out.query_ms.assign(nq, 0);
   out.status.assign(nq, GPSM_OK);
+  std::vector<uint32_t> dispatch(nq);
+  for (uint32_t k = 0; k < nq; ++k) dispatch[k] = k;
+  std::stable_sort(dispatch.begin(), dispatch.end(), [&](uint32_t a, uint32_t b) {
+    const uint64_t ma = q_eoff[a + 1] - q_eoff[a], mb = q_eoff[b + 1] - q_eoff[b];
+    if (ma != mb) return ma > mb;
+    return q_voff[a + 1] - q_voff[a] > q_voff[b + 1] - q_voff[b];
+  });
   std::atomic<uint32_t> next(0);
   std::atomic<int> first_error(GPSM_OK);
   std::mutex agg_mu;
@@ -101,8 +113,9 @@ int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const 
     Workspace& ws = *pool.ws[s];
     cudaEventRecord(e0[s], ws.stream);
     for (;;) {
-      const uint32_t k = next.fetch_add(1);
-      if (k >= nq) break;
+      const uint32_t slot_k = next.fetch_add(1);
+      if (slot_k >= nq) break;
+      const uint32_t k = dispatch[slot_k];
       const uint32_t qn = q_voff[k + 1] - q_voff[k];
       const uint32_t qm = (uint32_t)(q_eoff[k + 1] - q_eoff[k]);
       int rc;
@@ -190,6 +203,7 @@ struct Server {
   std::condition_variable cv_q, cv_done, cv_mem;
   std::deque<Request*> queue;
   std::map<uint64_t, Request*> all;
+  std::deque<uint64_t> finished;  // tickets in completion order (for wait_any)
   uint64_t next_id = 1;
   bool stopping = false;
   uint64_t budget = 0, in_use = 0, peak_in_use = 0;
@@ -274,6 +288,7 @@ struct Server {
         }
         r->t_end = now_ms();
         --active;
+        finished.push_back(r->id);
       }
       cv_done.notify_all();
     }
@@ -385,17 +400,10 @@ int gpsm_server_submit(gpsm_server_t h, uint32_t qn, const uint32_t* q_labels, u
 // Waits for a request (timeout_s < 0: forever); fills info and, when the
 // server collects rows and rows != NULL, a malloc'd copy of its rows
 // (free with gpsm_free) and its id_map (qn entries).
-int gpsm_server_wait(gpsm_server_t h, uint64_t ticket, double timeout_s, gpsm_request_info* info, uint32_t** rows,
-                     int32_t* id_map) {
-  if (!h) return GPSM_ERR_INVALID;
-  Server* S = h->s;
-  std::unique_lock<std::mutex> lk(S->mu);
-  auto it = S->all.find(ticket);
-  if (it == S->all.end()) return GPSM_ERR_INVALID;
+// Hands a finished request to the caller and forgets it (S->mu held).
+static int collect_request(Server* S, std::map<uint64_t, Request*>::iterator it, gpsm_request_info* info,
+                           uint32_t** rows, int32_t* id_map) {
   Request* r = it->second;
-  auto done = [&] { return r->status != 1; };
-  if (timeout_s < 0) S->cv_done.wait(lk, done);
-  else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done)) return GPSM_ERR_TIMEOUT;
   if (info) {
     memset(info, 0, sizeof(*info));
     info->status = r->status;
@@ -416,6 +424,41 @@ int gpsm_server_wait(gpsm_server_t h, uint64_t ticket, double timeout_s, gpsm_re
   S->all.erase(it);
   delete r;
   return st;
+}
+
+int gpsm_server_wait(gpsm_server_t h, uint64_t ticket, double timeout_s, gpsm_request_info* info, uint32_t** rows,
+                     int32_t* id_map) {
+  if (!h) return GPSM_ERR_INVALID;
+  Server* S = h->s;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  if (it == S->all.end()) return GPSM_ERR_INVALID;
+  Request* r = it->second;
+  auto done = [&] { return r->status != 1; };
+  if (timeout_s < 0) S->cv_done.wait(lk, done);
+  else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done)) return GPSM_ERR_TIMEOUT;
+  return collect_request(S, it, info, rows, id_map);
+}
+
+int gpsm_server_wait_any(gpsm_server_t h, double timeout_s, uint64_t* ticket, gpsm_request_info* info,
+                         uint32_t** rows, int32_t* id_map) {
+  if (!h || !ticket) return GPSM_ERR_INVALID;
+  Server* S = h->s;
+  std::unique_lock<std::mutex> lk(S->mu);
+  // finished tickets already collected by gpsm_server_wait are skipped
+  auto ready = [&] {
+    while (!S->finished.empty() && !S->all.count(S->finished.front())) S->finished.pop_front();
+    return !S->finished.empty() || S->all.empty();
+  };
+  if (timeout_s < 0) S->cv_done.wait(lk, ready);
+  else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) return GPSM_ERR_TIMEOUT;
+  if (S->finished.empty()) {
+    set_last_error("gpsm_server_wait_any: no request outstanding");
+    return GPSM_ERR_STATE;
+  }
+  *ticket = S->finished.front();
+  S->finished.pop_front();
+  return collect_request(S, S->all.find(*ticket), info, rows, id_map);
 }
 
 int gpsm_server_stats(gpsm_server_t h, uint64_t* in_use, uint64_t* peak_in_use, uint64_t* budget, uint32_t* queued,

@@ -350,6 +350,7 @@ int gpsm_set_tuning(const gpsm_tuning* t) {
   if (t->slots) T.slots = std::min<uint32_t>(t->slots, 64);
   if (t->race_share) T.race_share = t->race_share;
   if (t->scan_spin_limit) T.scan_spin_limit = t->scan_spin_limit;
+  if (t->ext_items) T.ext_items = t->ext_items >= 8 ? 8u : 4u;
   return GPSM_OK;
 }
 
@@ -363,6 +364,8 @@ int gpsm_get_tuning(gpsm_tuning* t) {
   t->slots = T.slots;
   t->scan_spin_limit = T.scan_spin_limit;
   t->race_share = T.race_share;
+  t->ext_items = T.ext_items;
+  t->pad = 0;
   return GPSM_OK;
 }
 

@@ -486,12 +486,20 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
   uint32_t* d_params = arena_alloc<uint32_t>(ws, params.size() + 1);
   if (!params.empty())
     GPSM_CUDA(cudaMemcpyAsync(d_params, params.data(), params.size() * 4, cudaMemcpyHostToDevice, s));
-  GPSM_CUDA(cudaStreamSynchronize(s));  // params is pageable host memory
+  uint32_t** d_lists = arena_alloc<uint32_t*>(ws, qn);
+  GPSM_CUDA(cudaMemcpyAsync(d_lists, list.data(), qn * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+  GPSM_CUDA(cudaStreamSynchronize(s));  // params and list are pageable host memory
 
   auto bm_of = [&](uint32_t u) { return bm + (size_t)u * W; };
   uint64_t launches = 0;
 
   // ---- candidate initialisation (match/Match.cu:661-719) ---------------------
+  // The reference collects C(u) into a list before each explore and refine
+  // step (kernel_collect); here those steps read C(u)'s bitmap directly, so
+  // only the final lists are compacted. An empty set stays empty (nothing
+  // adds candidates to u after its own step) and empties its neighbours' sets
+  // in refinement, so the final compaction reports it (DF_EMPTY), as the
+  // reference's early return does.
   for (uint32_t i = 0; i < Q.order.size(); ++i) {
     const uint32_t u = Q.order[i];
     if (!initialized[u]) {
@@ -501,45 +509,38 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
       ++launches;
       initialized[u] = 1;
     }
-    launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true);
-    ++launches;
     if (exp_cnt[i]) {
-      launch_explore(ws, g, list[u], counts + u, bound[u], u, d_params + exp_off[i], exp_cnt[i], bm);
+      launch_explore(ws, g, u, Q.lab[u], Q.deg(u), d_params + exp_off[i], exp_cnt[i], bm);
       ++launches;
     }
     for (uint32_t k = Q.roff[u]; k < Q.roff[u + 1]; ++k) initialized[Q.rcol[k]] = 1;
   }
-  // ---- refinement: 4 rounds + 1 emptiness check (match/Match.cu:848-890) ----
+  // ---- refinement: 4 rounds (match/Match.cu:848-890) -------------------------
   // Launches that would change nothing exit at once (RefineStamp): the
   // rounds and their order are the reference's, so the sets are the same.
+  // The reference's fifth round only collects (an emptiness check): the
+  // final compaction below does that.
   {
     uint32_t* stamp = arena_alloc<uint32_t>(ws, qn);
     GPSM_CUDA(cudaMemsetAsync(stamp, 0, sizeof(uint32_t) * qn, s));
-    std::vector<uint32_t> last_refine(qn, 0), last_compact(qn, 0);
+    std::vector<uint32_t> last_refine(qn, 0);
     uint32_t seq = 0;
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < 4; ++k)
       for (size_t i = 0; i < simple.size(); ++i) {
         const uint32_t u = simple[i];
-        // the first refinement-phase compaction of u always runs: explore
-        // may have removed candidates after u's compaction in the init loop
-        launch_compact(ws, bm_of(u), W, list[u], nullptr, counts + u, true, stamp, u, last_compact[u]);
-        last_compact[u] = seq;
-        ++launches;
-        if (k == 4 || ref_cnt[i] == 0) continue;
+        if (ref_cnt[i] == 0) continue;
         RefineStamp rs;
         rs.stamp = stamp;
         rs.prev = last_refine[u];
         rs.seq = ++seq;
-        launch_refine(ws, g, list[u], counts + u, bound[u], u, d_params + ref_off[i], ref_cnt[i], bm, rs);
+        launch_refine(ws, g, u, Q.lab[u], Q.deg(u), d_params + ref_off[i], ref_cnt[i], bm, rs);
         last_refine[u] = seq;
         ++launches;
       }
   }
-  // ---- final candidate lists with ranks -----------------------------------
-  for (uint32_t u = 0; u < qn; ++u) {
-    launch_compact(ws, bm_of(u), W, list[u], rank + (size_t)u * W, counts + u, true);
-    ++launches;
-  }
+  // ---- final candidate lists with ranks (one launch for every vertex) ------
+  launch_compact_multi(ws, bm, W, qn, d_lists, rank, counts);
+  ++launches;
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small, counts, qn * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 64, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
   GPSM_CUDA(cudaStreamSynchronize(s));
@@ -741,7 +742,8 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   js.coff = arena_alloc<unsigned long long>(ws, js.rows + 1);
   js.tiles = (opt.step_cands + join_cands_per_extend_tile() - 1) / join_cands_per_extend_tile() + 2;
   js.tile_row = arena_alloc<uint32_t>(ws, js.tiles);
-  js.kept = arena_alloc<uint2>(ws, js.tiles * join_cands_per_extend_tile());
+  js.kept_entries = js.tiles * join_cands_per_extend_tile() + join_kept_slack();
+  js.kept = arena_alloc<uint2>(ws, js.kept_entries);
   js.tile_cnt = arena_alloc<uint32_t>(ws, js.tiles);
   js.tile_off = arena_alloc<unsigned long long>(ws, js.tiles + 1);
   GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
@@ -1067,14 +1069,28 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
     // grow by 4 each round, until one finishes; the total work stays within
     // a small factor of the cheaper order's, so a plan the model got wrong
     // costs a bounded share instead of its whole blowup
+    // opt.work_cap bounds the query's candidates over all attempts together
     const std::vector<int32_t> learned_plan = pos2id;
     uint64_t share = tuning().race_share;
     for (uint32_t a = 0;; ++a) {
       const bool learned_turn = (a % 2) == 0;
       pos2id = learned_turn ? learned_plan : race;
-      const bool last = (opt.work_cap && share >= opt.work_cap) || share >= (1ull << 60);
+      uint64_t limit = share;
+      bool last = share >= (1ull << 60);
+      if (opt.work_cap) {
+        const uint64_t used = R.stats.cands_scanned;
+        const uint64_t left = opt.work_cap > used ? opt.work_cap - used : 0;
+        if (left <= share) {
+          limit = left;
+          last = true;
+        }
+        if (limit == 0) {  // the previous attempt used the whole cap: it stands, stopped
+          R.stats.aborted = true;
+          break;
+        }
+      }
       ++R.stats.order_attempts;
-      jrc = join_attempt(ctx, last ? opt.work_cap : share, hit);
+      jrc = join_attempt(ctx, limit, hit);
       if (jrc != GPSM_OK || !hit || last) {
         R.stats.aborted = hit;
         if (!learned_turn) R.stats.order_fallback = 3;

@@ -74,7 +74,7 @@ struct MatchOptions {
   bool directed = false;                // keep rows whose query edges exist as directed, labelled data edges
   std::vector<uint32_t> edge_labels;    // per query edge in file order (empty = all 1)
   uint64_t memory_budget = 0;           // bytes; predicted peak above it -> plain order (0 = arena size)
-  uint64_t work_cap = 0;                // candidates the joins may scan before stopping (0 = none)
+  uint64_t work_cap = 0;                // candidates the joins may scan before stopping, all attempts (0 = none)
   // Admission hook (serving): called after the order is chosen, before the
   // joins, with the bytes the joins are predicted to use; returns false to
   // refuse (GPSM_ERR_BUDGET). release() gets the same bytes back afterwards.

@@ -11,8 +11,8 @@
 // join order depends on the candidate-edge sizes they produce:
 //   k_mark_range   == check_kernel      (match/Match.cu:431-446)
 //   k_compact      == kernel_collect    (match/Match.cu:463-526)
-//   k_explore      == explore_kernel    (match/Match.cu:528-601)
-//   k_refine       == refine_kernel     (match/Match.cu:761-808)
+//   k_filter_step<true>  == kernel_collect + explore_kernel (match/Match.cu:528-601)
+//   k_filter_step<false> == kernel_collect + refine_kernel  (match/Match.cu:761-808)
 //   k_cedge_count  == count_kernel      (match/Match.cu:892-943)
 //   k_cedge_write  == examine_kernel    (match/Match.cu:961-1064)
 #include <cuda_runtime.h>
@@ -93,6 +93,66 @@ __global__ void __launch_bounds__(kCompactBlock) k_compact(const uint32_t* __res
   }
 }
 
+// The final candidate lists of query vertices 0..nverts-1 in one launch:
+// the block with ticket t compacts tile t % tiles_u of vertex t / tiles_u's
+// bitmap; each vertex's tiles are one look-back segment, so every vertex
+// gets its own sorted list, per-word ranks and count (DF_EMPTY when one is
+// empty), as nverts separate k_compact launches would.
+__global__ void __launch_bounds__(kCompactBlock) k_compact_multi(const uint32_t* __restrict__ bm, uint32_t words,
+                                                                uint32_t nverts, uint32_t* const* __restrict__ lists,
+                                                                uint32_t* __restrict__ rank,
+                                                                uint32_t* __restrict__ counts, Lookback lb) {
+  __shared__ uint32_t s_ticket;
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_ticket = lb_take_ticket(lb);
+  __syncthreads();
+  const uint32_t tiles_u = (words + kCompactWordsPerTile - 1) / kCompactWordsPerTile;
+  const uint32_t t = s_ticket;
+  if (t >= tiles_u * nverts) {  // ticket base out of step with the device counter
+    if (threadIdx.x == 0) atomicOr(lb.flags, (uint32_t)DF_BOUNDS);
+    return;
+  }
+  const uint32_t u = t / tiles_u, tile = t - u * tiles_u;
+  const uint32_t* bmu = bm + (size_t)u * words;
+  uint32_t* list = lists[u];
+  uint32_t* ranku = rank + (size_t)u * words;
+  const uint32_t w0 = tile * kCompactWordsPerTile + threadIdx.x * 4;
+  uint4 v = make_uint4(0, 0, 0, 0);
+  if (w0 < words) v = *reinterpret_cast<const uint4*>(bmu + w0);  // words is a multiple of 4
+  const uint32_t c0 = __popc(v.x), c1 = __popc(v.y), c2 = __popc(v.z), c3 = __popc(v.w);
+  unsigned long long total;
+  const unsigned long long mine = block_exclusive_scan<kCompactBlock>(c0 + c1 + c2 + c3, &total);
+  if (threadIdx.x < 32) {
+    const unsigned long long ex = lb_exclusive(lb, t, total, u * tiles_u);
+    if (threadIdx.x == 0) s_prefix = ex;
+  }
+  __syncthreads();
+  unsigned long long pos = s_prefix + mine;
+  if (w0 < words) {
+    uint4 r;
+    r.x = (uint32_t)pos;
+    r.y = (uint32_t)(pos + c0);
+    r.z = (uint32_t)(pos + c0 + c1);
+    r.w = (uint32_t)(pos + c0 + c1 + c2);
+    *reinterpret_cast<uint4*>(ranku + w0) = r;
+    const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      uint32_t x = wv[k];
+      while (x) {
+        const int b = __ffs(x) - 1;
+        x &= x - 1;
+        list[pos++] = (w0 + k) * 32 + b;
+      }
+    }
+  }
+  if (tile == tiles_u - 1 && threadIdx.x == 0) {
+    const unsigned long long c = s_prefix + total;
+    counts[u] = (uint32_t)c;
+    if (c == 0) atomicOr(lb.flags, (uint32_t)DF_EMPTY);
+  }
+}
+
 // Warp per candidate mu of u. For each target v (label, degree) in order:
 // every neighbour mv of mu with that label and degree >= deg(v) enters C(v);
 // if none does, mu leaves C(u) and later targets are skipped.
@@ -163,81 +223,85 @@ __device__ __forceinline__ const uint32_t* scan_range_block(const GraphView& g, 
   return scan_range_warp(g, mu, l, b, e, rb, re);
 }
 
-__global__ void __launch_bounds__(256) k_explore(GraphView g, const uint32_t* __restrict__ list,
-                                                 const uint32_t* __restrict__ count, uint32_t u,
-                                                 const uint32_t* __restrict__ tgt, uint32_t ntgt,
-                                                 uint32_t* __restrict__ bm, uint32_t words,
-                                                 const uint32_t* __restrict__ flags, HeavyList hl) {
-  extern __shared__ uint32_t s_tgt[];  // 3 * ntgt: v, label, degree
-  for (uint32_t i = threadIdx.x; i < 3 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
-  __syncthreads();
-  if (*flags & DF_EMPTY) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t n = *count;
-  uint32_t* bmu = bm + (size_t)u * words;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
-    const uint32_t mu = list[w];
-    const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    if (defer_heavy(e - b, mu, hl)) continue;
-    for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
-      uint32_t* bmv = bm + (size_t)v * words;
-      bool any = false;
-      uint32_t rb, re;
-      const uint32_t* cl = scan_range_warp(g, mu, lv, b, e, &rb, &re);
-      for (uint32_t j = rb + lane; j < re; j += 32) {
-        const uint32_t mv = cl[j];
-        const uint2 ld = g.labdeg[mv];
-        if (ld.x == lv && ld.y >= dv) {
-          atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
-          any = true;
-        }
+// ---- exploration and refinement: one launch per query vertex --------------
+// Candidates of u are read from C(u)'s bitmap (no compaction before each
+// step): warps of the first `light_blocks` blocks take chunks of `cw` words
+// (1..32, so that small bitmaps still spread over thousands of warps) and
+// handle their candidates one at a time with lanes over
+// neighbours; a candidate with more than `hub_degree` neighbours (a hub) is
+// left to the remaining blocks of the same launch, which walk the hubs of
+// u's label (a prefix of lab_vtx, degree descending) with threads over
+// neighbours. Same candidates, same per-candidate steps, so the sets are
+// those of the reference's collect + explore / refine sequence.
+struct StepTargets {
+  const uint32_t* tgt;  // explore: (v, label, degree) per target; refine: (x, label)
+  uint32_t ntgt;
+};
+
+// Explore one candidate mu of u, cooperatively over `group` threads
+// (a warp or a block): every neighbour mv with the target's label and
+// degree >= the target's enters C(v); mu leaves C(u) at the first target
+// that gets none (match/Match.cu:594-598) and later targets are skipped.
+template <bool BLOCK>
+__device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
+                                            const uint32_t* s_tgt, uint32_t ntgt, uint32_t* __restrict__ bm,
+                                            uint32_t words, uint32_t* bmu) {
+  const uint32_t tid = BLOCK ? threadIdx.x : (threadIdx.x & 31);
+  const uint32_t nthr = BLOCK ? blockDim.x : 32;
+  for (uint32_t t = 0; t < ntgt; ++t) {
+    const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
+    uint32_t* bmv = bm + (size_t)v * words;
+    bool any = false;
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_warp(g, mu, lv, b, e, &rb, &re);
+    for (uint32_t j = rb + tid; j < re; j += nthr) {
+      const uint32_t mv = cl[j];
+      const uint2 ld = g.labdeg[mv];
+      if (ld.x == lv && ld.y >= dv) {
+        atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
+        any = true;
       }
-      if (!__any_sync(0xffffffffu, any)) {
-        if (lane == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
-        break;
-      }
+    }
+    const bool got = BLOCK ? __syncthreads_or(any) : __any_sync(0xffffffffu, any);
+    if (!got) {
+      if (tid == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+      return;
     }
   }
 }
 
-// Block per deferred candidate: the same steps as k_explore with a
-// block-wide vote per target.
-__global__ void __launch_bounds__(kHeavyBlock) k_explore_heavy(GraphView g, HeavyList hl, uint32_t u,
-                                                               const uint32_t* __restrict__ tgt, uint32_t ntgt,
-                                                               uint32_t* __restrict__ bm, uint32_t words,
-                                                               const uint32_t* __restrict__ flags) {
-  if (*flags & DF_EMPTY) return;
-  const uint32_t n = min(*hl.count, hl.cap);
-  uint32_t* bmu = bm + (size_t)u * words;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const uint32_t mu = hl.items[i];
-    const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t v = tgt[3 * t], lv = tgt[3 * t + 1], dv = tgt[3 * t + 2];
-      uint32_t* bmv = bm + (size_t)v * words;
-      bool any = false;
-      uint32_t rb, re;
-      const uint32_t* cl = scan_range_block(g, mu, lv, b, e, &rb, &re);
-      for (uint32_t j = rb + threadIdx.x; j < re; j += blockDim.x) {
+// Refine one candidate mu of u over `group` threads: mu stays only if every
+// target x has a candidate among mu's neighbours (match/Match.cu:761-808).
+template <bool BLOCK>
+__device__ __forceinline__ void refine_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
+                                           const uint32_t* s_tgt, uint32_t ntgt, const uint32_t* __restrict__ bm,
+                                           uint32_t words, uint32_t* bmu, const RefineStamp& rs, uint32_t u) {
+  const uint32_t tid = BLOCK ? threadIdx.x : (threadIdx.x & 31);
+  const uint32_t nthr = BLOCK ? blockDim.x : 32;
+  for (uint32_t t = 0; t < ntgt; ++t) {
+    const uint32_t* bmv = bm + (size_t)s_tgt[2 * t] * words;
+    bool found = false;
+    uint32_t rb, re;
+    const uint32_t* cl = scan_range_warp(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
+    for (uint32_t j0 = rb; j0 < re && !found; j0 += nthr) {
+      const uint32_t j = j0 + tid;
+      bool hit = false;
+      if (j < re) {
         const uint32_t mv = cl[j];
-        const uint2 ld = g.labdeg[mv];
-        if (ld.x == lv && ld.y >= dv) {
-          atomicOr(&bmv[mv >> 5], 1u << (mv & 31));
-          any = true;
-        }
+        hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
       }
-      if (!__syncthreads_or(any)) {
-        if (threadIdx.x == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
-        break;
+      found = BLOCK ? __syncthreads_or(hit) : __any_sync(0xffffffffu, hit);
+    }
+    if (!found) {
+      if (tid == 0) {
+        atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+        if (rs.stamp) rs.stamp[u] = rs.seq;
       }
+      return;
     }
   }
 }
 
-// Warp per candidate mu of u: mu stays only if every target v has a
-// candidate among mu's neighbours.
 // True when no target's candidate set changed since u's previous refinement.
 __device__ __forceinline__ bool refine_is_noop(const RefineStamp& rs, const uint32_t* tgt, uint32_t ntgt) {
   if (rs.prev == 0) return false;
@@ -246,85 +310,53 @@ __device__ __forceinline__ bool refine_is_noop(const RefineStamp& rs, const uint
   return true;
 }
 
-__global__ void __launch_bounds__(256) k_refine(GraphView g, const uint32_t* __restrict__ list,
-                                                const uint32_t* __restrict__ count, uint32_t u,
-                                                const uint32_t* __restrict__ tgt, uint32_t ntgt,
-                                                uint32_t* __restrict__ bm, uint32_t words,
-                                                const uint32_t* __restrict__ flags, HeavyList hl, RefineStamp rs) {
-  extern __shared__ uint32_t s_tgt[];  // 2 * ntgt: x, label
-  for (uint32_t i = threadIdx.x; i < 2 * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
+// EXPLORE: explore_one; otherwise refine_one. hubs: [hub_begin, hub_end) of
+// lab_vtx, the vertices of u's label with more than hub_degree neighbours.
+template <bool EXPLORE>
+__global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint32_t* __restrict__ lab_vtx,
+                                                     uint32_t hub_begin, uint32_t hub_end, uint32_t hub_degree,
+                                                     uint32_t light_blocks, uint32_t cw, uint32_t u,
+                                                     const uint32_t* __restrict__ tgt, uint32_t ntgt,
+                                                     uint32_t* __restrict__ bm, uint32_t words,
+                                                     const uint32_t* __restrict__ flags, RefineStamp rs) {
+  constexpr uint32_t kStride = EXPLORE ? 3 : 2;
+  extern __shared__ uint32_t s_tgt[];
+  for (uint32_t i = threadIdx.x; i < kStride * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
   if (*flags & DF_EMPTY) return;
-  if (refine_is_noop(rs, s_tgt, ntgt)) return;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t n = *count;
+  if (!EXPLORE && refine_is_noop(rs, s_tgt, ntgt)) return;
   uint32_t* bmu = bm + (size_t)u * words;
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
-    const uint32_t mu = list[w];
-    const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    if (defer_heavy(e - b, mu, hl)) continue;
-    for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t* bmv = bm + (size_t)s_tgt[2 * t] * words;
-      bool found = false;
-      uint32_t rb, re;
-      const uint32_t* cl = scan_range_warp(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
-      for (uint32_t j0 = rb; j0 < re; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        bool hit = false;
-        if (j < re) {
-          const uint32_t mv = cl[j];
-          hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+  if (blockIdx.x < light_blocks) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nwarps = light_blocks * (blockDim.x >> 5);
+    for (uint32_t c0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * cw; c0 < words; c0 += nwarps * cw) {
+      // each word of the chunk belongs to this warp alone: only its own
+      // candidates' bits are cleared while it runs
+      const uint32_t wv = (lane < cw && c0 + lane < words) ? bmu[c0 + lane] : 0u;
+      uint32_t pending = __ballot_sync(0xffffffffu, wv != 0);
+      while (pending) {
+        const uint32_t src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        uint32_t word = __shfl_sync(0xffffffffu, wv, src);
+        while (word) {
+          const uint32_t mu = (c0 + src) * 32 + (__ffs(word) - 1);
+          word &= word - 1;
+          const uint32_t b = g.off[mu], e = g.off[mu + 1];
+          if (e - b > hub_degree) continue;  // a hub: the hub blocks take it
+          if (EXPLORE) explore_one<false>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
+          else refine_one<false>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
         }
-        if (__any_sync(0xffffffffu, hit)) {
-          found = true;
-          break;
-        }
-      }
-      if (!found) {
-        if (lane == 0) {
-          atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
-          if (rs.stamp) rs.stamp[u] = rs.seq;
-        }
-        break;
       }
     }
+    return;
   }
-}
-
-__global__ void __launch_bounds__(kHeavyBlock) k_refine_heavy(GraphView g, HeavyList hl, uint32_t u,
-                                                              const uint32_t* __restrict__ tgt, uint32_t ntgt,
-                                                              uint32_t* __restrict__ bm, uint32_t words,
-                                                              const uint32_t* __restrict__ flags, RefineStamp rs) {
-  if (*flags & DF_EMPTY) return;
-  if (refine_is_noop(rs, tgt, ntgt)) return;
-  const uint32_t n = min(*hl.count, hl.cap);
-  uint32_t* bmu = bm + (size_t)u * words;
-  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const uint32_t mu = hl.items[i];
+  for (uint32_t i = hub_begin + (blockIdx.x - light_blocks); i < hub_end; i += gridDim.x - light_blocks) {
+    const uint32_t mu = lab_vtx[i];
+    if (!((bmu[mu >> 5] >> (mu & 31)) & 1u)) continue;  // not (or no longer) a candidate of u
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    for (uint32_t t = 0; t < ntgt; ++t) {
-      const uint32_t* bmv = bm + (size_t)tgt[2 * t] * words;
-      bool found = false;
-      uint32_t rb, re;
-      const uint32_t* cl = scan_range_block(g, mu, tgt[2 * t + 1], b, e, &rb, &re);
-      for (uint32_t j0 = rb; j0 < re && !found; j0 += blockDim.x) {
-        const uint32_t j = j0 + threadIdx.x;
-        bool hit = false;
-        if (j < re) {
-          const uint32_t mv = cl[j];
-          hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
-        }
-        found = __syncthreads_or(hit);
-      }
-      if (!found) {
-        if (threadIdx.x == 0) {
-          atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
-          if (rs.stamp) rs.stamp[u] = rs.seq;
-        }
-        break;
-      }
-    }
+    if (EXPLORE) explore_one<true>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
+    else refine_one<true>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
+    __syncthreads();  // the bitmap word read above is read again for the next hub
   }
 }
 
@@ -575,6 +607,14 @@ void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t*
   GPSM_LAUNCHED();
 }
 
+void launch_compact_multi(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t nverts, uint32_t* const* d_lists,
+                          uint32_t* rank, uint32_t* counts) {
+  const uint32_t tiles = ((words + kCompactWordsPerTile - 1) / kCompactWordsPerTile) * nverts;
+  Lookback lb = make_lb(ws, tiles);
+  k_compact_multi<<<tiles, kCompactBlock, 0, ws.stream>>>(bm, words, nverts, d_lists, rank, counts, lb);
+  GPSM_LAUNCHED();
+}
+
 static HeavyList heavy_list(Workspace& ws, const DeviceGraph& g) {
   HeavyList hl;
   hl.threshold = std::max<uint32_t>(tuning().heavy_degree, 32);
@@ -586,34 +626,39 @@ static HeavyList heavy_list(Workspace& ws, const DeviceGraph& g) {
   return hl;
 }
 
-void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                    uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
-  if (ntgt == 0 || max_count == 0) return;
-  HeavyList hl = heavy_list(ws, g);
-  uint32_t blocks = grid_for(max_count, 148 * 16);
-  k_explore<<<blocks, 256, 3 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm,
-                                                                    g.words, ws.d_flags, hl);
-  GPSM_LAUNCHED();
-  if (hl.items) {
-    k_explore_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags);
-    GPSM_LAUNCHED();
-  }
+// Words per warp chunk of a bitmap of `words` words: about 8192 warps (a
+// full B200 holds 148 x 64), at most 32 words (one per lane) a chunk.
+static uint32_t chunk_words(uint32_t words) { return std::max<uint32_t>(1, std::min<uint32_t>(32, (words + 8191) / 8192)); }
+
+// Blocks of 8 warps that cover the bitmap in chunks of chunk_words(words).
+static uint32_t light_blocks_for(uint32_t words) {
+  const uint32_t cw = chunk_words(words);
+  const uint32_t chunks = (words + cw - 1) / cw;
+  return std::max<uint32_t>(1, std::min<uint32_t>((chunks + 7) / 8, 148 * 16));
 }
 
-void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm,
-                   RefineStamp rs) {
-  if (ntgt == 0 || max_count == 0) return;
-  HeavyList hl = heavy_list(ws, g);
-  uint32_t blocks = grid_for(max_count, 148 * 16);
-  k_refine<<<blocks, 256, 2 * ntgt * sizeof(uint32_t), ws.stream>>>(view(g), list, count, u, tgt, ntgt, bm, g.words,
-                                                               ws.d_flags, hl, rs);
+template <bool EXPLORE>
+static void launch_filter_step(Workspace& ws, const DeviceGraph& g, uint32_t u, uint32_t lab_u, uint32_t deg_u,
+                               const uint32_t* tgt, uint32_t ntgt, uint32_t* bm, RefineStamp rs) {
+  if (ntgt == 0) return;
+  const uint32_t hub = std::max<uint32_t>(tuning().heavy_degree, 32);
+  uint32_t hb = 0, he = 0;
+  if (g.max_degree > hub) g.label_range(lab_u, std::max(hub + 1, deg_u), &hb, &he);
+  const uint32_t light = light_blocks_for(g.words);
+  const uint32_t hubs = std::min<uint32_t>(he - hb, (uint32_t)sm_count() * 2);
+  k_filter_step<EXPLORE><<<light + hubs, 256, (EXPLORE ? 3 : 2) * ntgt * sizeof(uint32_t), ws.stream>>>(
+      view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
   GPSM_LAUNCHED();
-  if (hl.items) {
-    k_refine_heavy<<<sm_count() * 2, kHeavyBlock, 0, ws.stream>>>(view(g), hl, u, tgt, ntgt, bm, g.words, ws.d_flags,
-                                                                  rs);
-    GPSM_LAUNCHED();
-  }
+}
+
+void launch_explore(Workspace& ws, const DeviceGraph& g, uint32_t u, uint32_t lab_u, uint32_t deg_u,
+                    const uint32_t* tgt, uint32_t ntgt, uint32_t* bm) {
+  launch_filter_step<true>(ws, g, u, lab_u, deg_u, tgt, ntgt, bm, RefineStamp());
+}
+
+void launch_refine(Workspace& ws, const DeviceGraph& g, uint32_t u, uint32_t lab_u, uint32_t deg_u,
+                   const uint32_t* tgt, uint32_t ntgt, uint32_t* bm, RefineStamp rs) {
+  launch_filter_step<false>(ws, g, u, lab_u, deg_u, tgt, ntgt, bm, rs);
 }
 
 void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,

@@ -59,11 +59,17 @@ void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint
 void launch_compact(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t* list, uint32_t* rank,
                     uint32_t* count, bool set_empty_flag, const uint32_t* stamp = nullptr, uint32_t u = 0,
                     uint32_t prev = 0);
-void launch_explore(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                    uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
-void launch_refine(Workspace& ws, const DeviceGraph& g, const uint32_t* list, const uint32_t* count,
-                   uint32_t max_count, uint32_t u, const uint32_t* tgt, uint32_t ntgt, uint32_t* bm,
-                   RefineStamp rs = RefineStamp());
+// Exploration and refinement of query vertex u (label lab_u, query degree
+// deg_u) over the candidates in u's bitmap, hubs included, in one launch.
+// tgt: explore (v, label, degree) per target; refine (x, label) per target.
+// Final lists, ranks and counts of the bitmaps of vertices 0..nverts-1 in one
+// launch (d_lists: device array of nverts list pointers; rank: nverts x words).
+void launch_compact_multi(Workspace& ws, const uint32_t* bm, uint32_t words, uint32_t nverts, uint32_t* const* d_lists,
+                          uint32_t* rank, uint32_t* counts);
+void launch_explore(Workspace& ws, const DeviceGraph& g, uint32_t u, uint32_t lab_u, uint32_t deg_u,
+                    const uint32_t* tgt, uint32_t ntgt, uint32_t* bm);
+void launch_refine(Workspace& ws, const DeviceGraph& g, uint32_t u, uint32_t lab_u, uint32_t deg_u,
+                   const uint32_t* tgt, uint32_t ntgt, uint32_t* bm, RefineStamp rs = RefineStamp());
 // d_base[ndir+1]: first work item of each direction, d_base[ndir] = items
 void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_dirs, uint32_t ndir,
                         const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt);
@@ -105,14 +111,18 @@ struct JoinScratch {
   uint4* rng = nullptr;               // rows x nb list ranges (lo, lo>>32, length, 0)
   unsigned long long* coff = nullptr;
   uint32_t* tile_row = nullptr;       // per extend tile: the row holding its first candidate
-  uint2* kept = nullptr;              // tiles x 1024: kept (row, new value) of each tile, in order
+  uint2* kept = nullptr;              // per tile (256 x items): kept (row, new value) of each tile, in order
   uint32_t* tile_cnt = nullptr;       // kept candidates per tile
   unsigned long long* tile_off = nullptr;  // tiles + 1: output row of each tile's first kept candidate
   uint64_t rows = 0;
   uint64_t rng_entries = 0;
   uint64_t tiles = 0;                 // entries of tile_row
+  uint64_t kept_entries = 0;          // entries of kept
 };
+// Candidates of the smallest check tile (sizes tile counts) and the extra
+// kept entries that cover rounding the budget up to the largest tile.
 uint64_t join_cands_per_extend_tile();
+uint64_t join_kept_slack();
 
 // One join step over input rows [row_begin, row_end) (in_cols columns,
 // row-major): rows are admitted in order while their candidates fit

@@ -112,6 +112,9 @@ struct Tuning {
   // polls of one predecessor's status a look-back makes before giving up
   // (DF_SCAN_TIMEOUT): the bound on every inter-block wait
   uint32_t scan_spin_limit = 1u << 22;
+  // candidates per thread of the join check kernel (4 or 8): its tile is
+  // 256 x ext_items candidates
+  uint32_t ext_items = 4;
 };
 Tuning& tuning();
 int sm_count();

@@ -18,12 +18,16 @@
 //                   lengths into candidate offsets with a single-pass
 //                   decoupled look-back scan. Rows are admitted in order while
 //                   their candidates fit the step budget.
-//   k_extend_check  (persistent blocks, tiles of 1024 candidates) takes
-//                   candidate t of row r from the driver list and keeps it if
-//                   it differs from every value in the row that could repeat
-//                   (injectivity) and lies in every other placed neighbour's
-//                   list (binary search: sorted-list intersection). Each tile
-//                   writes its kept (row, value) pairs in order and its count.
+//   k_extend_check  (persistent blocks, tiles of 256 x ITEMS candidates)
+//                   takes candidate t of row r from the driver list and keeps
+//                   it if it differs from every value in the row that could
+//                   repeat (injectivity) and lies in every other placed
+//                   neighbour's list (sorted-list intersection). A thread
+//                   takes ITEMS consecutive candidates: ascending values of
+//                   one row (mostly), so the row's state is loaded once and
+//                   each list is searched from where the previous value was
+//                   found (galloping), not from its start. Each tile writes
+//                   its kept (row, value) pairs in order and its count.
 //   k_scan_u32      turns the tile counts into output offsets.
 //   k_extend_write  copies each tile's kept rows (input row + new value) to
 //                   its offset: one contiguous, coalesced span per tile.
@@ -44,24 +48,36 @@ namespace gpsm {
 
 constexpr int kLocBlock = 256;  // rows per locate tile
 constexpr int kExtBlock = 256;
-constexpr int kExtItems = 4;
-constexpr int kExtTile = kExtBlock * kExtItems;  // candidates per extend tile
-static uint32_t ext_resident_per_sm();
-static uint32_t ext_grid() {  // persistent extend blocks: all resident at once
-  const uint32_t per_sm = std::min<uint32_t>(std::max<uint32_t>(1, tuning().ext_blocks_per_sm), ext_resident_per_sm());
-  return (uint32_t)sm_count() * per_sm;
-}
+constexpr uint32_t kMinExtTile = kExtBlock * 4;   // tiles are 256 x {4, 8} candidates
+constexpr uint32_t kMaxExtTile = kExtBlock * 8;
+constexpr int kInjReg = 8;  // injectivity columns a thread holds in registers per row
 
-__device__ __forceinline__ bool sorted_contains(const uint32_t* __restrict__ a, unsigned long long lo,
-                                                unsigned long long hi, uint32_t key) {
+// Candidates per check thread of the next step (tuning; 4 or 8).
+static uint32_t ext_items() { return tuning().ext_items >= 8 ? 8u : 4u; }
+
+// First index in a[lo, hi) whose value is >= key (hi when none).
+__device__ __forceinline__ unsigned long long lower_bound_u32(const uint32_t* __restrict__ a, unsigned long long lo,
+                                                              unsigned long long hi, uint32_t key) {
   while (lo < hi) {
     const unsigned long long mid = (lo + hi) >> 1;
-    const uint32_t x = __ldg(a + mid);
-    if (x == key) return true;
-    if (x < key) lo = mid + 1;
+    if (__ldg(a + mid) < key) lo = mid + 1;
     else hi = mid;
   }
-  return false;
+  return lo;
+}
+
+// The same, given that every value before lo is < key: probes lo, lo+1,
+// lo+3, lo+7, ... until a value >= key, then a binary search inside the last
+// gap; O(log d) for an answer d places after lo.
+__device__ __forceinline__ unsigned long long gallop_u32(const uint32_t* __restrict__ a, unsigned long long lo,
+                                                         unsigned long long hi, uint32_t key) {
+  unsigned long long step = 1, probe = lo;
+  while (probe < hi && __ldg(a + probe) < key) {
+    lo = probe + 1;
+    probe = lo + step;
+    step <<= 1;
+  }
+  return lower_bound_u32(a, lo, min(probe, hi), key);
 }
 
 // Candidate-edge list of data vertex mu (a candidate of w) towards v.
@@ -96,7 +112,7 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
                                                      uint4* __restrict__ drv, uint4* __restrict__ rng,
                                                      unsigned long long* __restrict__ coff,
                                                      uint32_t* __restrict__ tile_row, unsigned long long tile_cap,
-                                                     StepState* __restrict__ st, Lookback lb) {
+                                                     uint32_t ext_tile, StepState* __restrict__ st, Lookback lb) {
   __shared__ LocateShared S;
   __shared__ uint32_t s_skip;
   if (threadIdx.x == 0) {
@@ -157,8 +173,8 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
     if (i + 1 == nrows) coff[nrows] = off + best_len;
     // extend tiles whose first candidate lies in this row start at this row
     if (best_len > 0)
-      for (unsigned long long T = (off + kExtTile - 1) / kExtTile;
-           T * kExtTile < off + best_len && T < tile_cap; ++T)
+      for (unsigned long long T = (off + ext_tile - 1) / ext_tile;
+           T * ext_tile < off + best_len && T < tile_cap; ++T)
         tile_row[T] = (uint32_t)i;
   }
   if (nfit > 0 && threadIdx.x == (uint32_t)nfit - 1) {
@@ -169,7 +185,7 @@ __global__ void __launch_bounds__(kLocBlock) k_locate(const uint32_t* __restrict
   if (threadIdx.x == 0 && (unsigned long long)nfit < in_tile) atomicExch(&st->full, 1ULL);
 }
 
-constexpr uint32_t kSpan = 1024;  // rows of one tile whose offsets are staged in shared memory
+constexpr uint32_t kSpan = kMaxExtTile;  // rows of one tile whose offsets are staged in shared memory
 
 struct ExtendShared {
   BackNbr back[kMaxBack];
@@ -177,7 +193,6 @@ struct ExtendShared {
   uint32_t tile;
   unsigned long long r0, r1;  // rows holding the tile's first and (at most) last candidate
   uint32_t warp_sum[kExtBlock / 32];  // kept candidates per warp, then their exclusive prefix
-  uint32_t total;                     // kept candidates of the tile
   unsigned long long coff[kSpan + 1];
 };
 
@@ -193,22 +208,19 @@ __device__ __forceinline__ unsigned long long row_of(const unsigned long long* _
   return lo;
 }
 
-// Injectivity: y differs from the row's columns that hold a query vertex
-// with the new vertex's label (a data vertex has one label, so y can only
-// repeat such a column).
-__device__ __forceinline__ bool injective(const ExtendShared& S, const uint32_t* __restrict__ row, uint32_t ninj,
-                                          uint32_t y) {
-  for (uint32_t c = 0; c < ninj; ++c)
-    if (__ldg(row + S.inj[c]) == y) return false;
-  return true;
-}
-
-// Persistent blocks take tiles of kExtTile consecutive candidates from a
-// counter. Thread i of a block takes candidates 4i .. 4i+3 of the tile: one
-// row search for the first, the next ones usually in the same row (its
-// driver range and row pointer are loaded once per row). The tile's kept
-// candidates go to kept[tile * kExtTile ...] in candidate order, their
-// number to tile_cnt[tile].
+// Persistent blocks take tiles of 256 x ITEMS consecutive candidates from a
+// counter. Thread i of a block takes candidates ITEMS*i .. ITEMS*i+ITEMS-1
+// of the tile, in two passes:
+//   1. per candidate: its row (one search for the first, then the next
+//      rows in order), its value y, the parallel-edge repeat check and
+//      injectivity against the row's same-label columns, which are loaded
+//      into registers once per row;
+//   2. per other placed neighbour j: every surviving candidate is looked up
+//      in that neighbour's list. Values of one row ascend, so the search
+//      for the next candidate starts where the previous one ended.
+// The tile's kept candidates go to kept[tile * tile_size ...] in candidate
+// order, their number to tile_cnt[tile].
+template <int ITEMS>
 __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
                                                            unsigned long long row_begin,
                                                            const BackNbr* __restrict__ back, uint32_t nb,
@@ -219,6 +231,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
                                                            uint2* __restrict__ kept, uint32_t* __restrict__ tile_cnt,
                                                            StepState* __restrict__ st,
                                                            const uint32_t* __restrict__ inj, uint32_t ninj) {
+  constexpr uint32_t kTile = kExtBlock * ITEMS;
   __shared__ ExtendShared S;
   stage_back(S.back, back, nb);
   for (uint32_t i = threadIdx.x; i < ninj; i += blockDim.x) S.inj[i] = inj[i];
@@ -226,7 +239,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
   const unsigned long long nr = st->rows;     // rows admitted by k_locate
   // coff[nr] may lie in a tile k_locate skipped; the admitted rows' end is exact
   const unsigned long long ncand = nr ? st->cand_end : 0;
-  const unsigned long long ntiles = (ncand + kExtTile - 1) / kExtTile;
+  const unsigned long long ntiles = (ncand + kTile - 1) / kTile;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cands = ncand;
   for (;;) {
     __syncthreads();  // the previous tile's shared state is no longer read
@@ -243,19 +256,19 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
     __syncthreads();
     const uint32_t tile = S.tile;
     if ((unsigned long long)tile >= ntiles) break;
-    const unsigned long long t_first = (unsigned long long)tile * kExtTile;
-    const unsigned long long t_end = min(t_first + kExtTile, ncand);
+    const unsigned long long t_first = (unsigned long long)tile * kTile;
+    const unsigned long long t_end = min(t_first + kTile, ncand);
     const unsigned long long r0 = S.r0, span = S.r1 - S.r0 + 1;
     const bool staged = span <= kSpan;
     if (staged)
       for (uint32_t x = threadIdx.x; x <= span; x += blockDim.x)
         S.coff[x] = r0 + x < nr ? __ldg(coff + r0 + x) : ncand;
     __syncthreads();
-    uint32_t kr[kExtItems], ky[kExtItems];  // item k's row and value (valid where keep has bit k)
+    uint32_t kr[ITEMS], ky[ITEMS], kd[ITEMS];  // item k's row, value and driver list index
     uint32_t keep = 0;
-    const unsigned long long tb = t_first + (unsigned long long)threadIdx.x * kExtItems;
+    const unsigned long long tb = t_first + (unsigned long long)threadIdx.x * ITEMS;
     if (tb < t_end) {
-      // row of candidate tb: the last row whose first candidate is <= tb
+      // pass 1: rows, values, repeats and injectivity
       unsigned long long r, rstart, rend;
       uint32_t li = 0;
       if (staged) {
@@ -278,13 +291,19 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
       unsigned long long lo = ((unsigned long long)d.y << 32) | d.x;
       const uint32_t* __restrict__ nbrs = S.back[d.w].nbrs;
       const uint32_t* row = in + (row_begin + r) * cols;
+      uint32_t injv[kInjReg];
+#pragma unroll
+      for (int c = 0; c < kInjReg; ++c) injv[c] = (uint32_t)c < ninj ? __ldg(row + S.inj[c]) : 0u;
       uint32_t prev = 0;
       bool has_prev = tb > rstart;  // parallel data edges: each neighbour once
       if (has_prev) prev = __ldg(nbrs + lo + (tb - rstart) - 1);
 #pragma unroll
-      for (int k = 0; k < kExtItems; ++k) {
+      for (int k = 0; k < ITEMS; ++k) {
         const unsigned long long t = tb + k;
-        if (t >= t_end) break;
+        kr[k] = (uint32_t)r;
+        ky[k] = 0;
+        kd[k] = d.w;
+        if (t >= t_end) continue;
         while (t >= rend) {  // the next row with candidates
           ++r;
           if (staged) {
@@ -299,23 +318,41 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
           lo = ((unsigned long long)d.y << 32) | d.x;
           nbrs = S.back[d.w].nbrs;
           row = in + (row_begin + r) * cols;
+#pragma unroll
+          for (int c = 0; c < kInjReg; ++c) injv[c] = (uint32_t)c < ninj ? __ldg(row + S.inj[c]) : 0u;
           has_prev = false;
         }
         const uint32_t y = __ldg(nbrs + lo + (t - rstart));
         bool ok = !(has_prev && prev == y);
         prev = y;
         has_prev = true;
-        if (ok) ok = injective(S, row, ninj, y);
-        // y must lie in every other placed neighbour's list
-        for (uint32_t j = 0; ok && j < nb; ++j) {
-          if (j == d.w) continue;
-          const uint4 g2 = __ldg(rng + r * nb + j);
-          const unsigned long long l2 = ((unsigned long long)g2.y << 32) | g2.x;
-          ok = sorted_contains(S.back[j].nbrs, l2, l2 + g2.z, y);
-        }
+#pragma unroll
+        for (int c = 0; c < kInjReg; ++c) ok = ok && !((uint32_t)c < ninj && injv[c] == y);
+        for (uint32_t c = kInjReg; ok && c < ninj; ++c) ok = __ldg(row + S.inj[c]) != y;
         kr[k] = (uint32_t)r;
         ky[k] = y;
+        kd[k] = d.w;
         keep |= (ok ? 1u : 0u) << k;
+      }
+      // pass 2: y must lie in every other placed neighbour's list
+      for (uint32_t j = 0; keep && j < nb; ++j) {
+        const uint32_t* __restrict__ list = S.back[j].nbrs;
+        uint32_t cur = 0xffffffffu;
+        unsigned long long pos = 0, hi = 0;
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+          if (!((keep >> k) & 1u) || kd[k] == j) continue;
+          if (kr[k] != cur) {  // first candidate of this row in this list: search the whole range
+            cur = kr[k];
+            const uint4 g2 = __ldg(rng + (unsigned long long)cur * nb + j);
+            pos = ((unsigned long long)g2.y << 32) | g2.x;
+            hi = pos + g2.z;
+            pos = lower_bound_u32(list, pos, hi, ky[k]);
+          } else {
+            pos = gallop_u32(list, pos, hi, ky[k]);
+          }
+          if (!(pos < hi && __ldg(list + pos) == ky[k])) keep &= ~(1u << k);
+        }
       }
     }
     // in-tile positions: warp inclusive scan of the per-thread counts, then
@@ -341,24 +378,25 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
       if (lane == 31) tile_cnt[tile] = x;
     }
     __syncthreads();
-    uint2* dst = kept + (unsigned long long)tile * kExtTile + S.warp_sum[wid] + incl - cnt;
+    uint2* dst = kept + (unsigned long long)tile * kTile + S.warp_sum[wid] + incl - cnt;
 #pragma unroll
-    for (int k = 0; k < kExtItems; ++k)
+    for (int k = 0; k < ITEMS; ++k)
       if (keep & (1u << k)) *dst++ = make_uint2(kr[k], ky[k]);
   }
 }
 
 // Block per tile (grid-stride): the tile's kept rows go to output rows
 // tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
-// written.
-__global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
+// written. Every load a lane issues for a group of rows is issued before
+// its stores, so each lane has kU kept pairs, then kU input words, in flight.
+__global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
                                                       unsigned long long row_begin, const uint2* __restrict__ kept,
                                                       const uint32_t* __restrict__ tile_cnt,
                                                       const unsigned long long* __restrict__ tile_off,
-                                                      uint32_t ntiles_max, uint32_t* __restrict__ out,
+                                                      uint32_t ntiles_max, uint32_t ext_tile, uint32_t* __restrict__ out,
                                                       unsigned long long out_cap, StepState* __restrict__ st) {
+  constexpr int kU = 8;
   const uint32_t out_cols = cols + 1;
-  const float inv_out_cols = 1.0f / (float)out_cols;
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   // rows of at most 32 words: lane -> (row within a group of rpw rows, column)
   const uint32_t rpw = out_cols <= 32 ? 32 / out_cols : 0;
@@ -369,12 +407,9 @@ __global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict
     const uint32_t c = tile_cnt[tile];
     const unsigned long long o = tile_off[tile];
     if (c == 0 || o >= out_cap) continue;
-    const uint2* kt = kept + (unsigned long long)tile * kExtTile;
+    const uint2* kt = kept + (unsigned long long)tile * ext_tile;
     if (rpw) {
-      // each warp writes rpw whole rows per step (one contiguous span), four
-      // steps at a time: all loads are issued before the stores, so a lane
-      // has four kept pairs and then four input words in flight
-      constexpr int kU = 4;
+      // each warp writes rpw whole rows per store (one contiguous span)
       const uint32_t stride = nwarps * rpw;
       for (uint32_t qb = wid * rpw; qb < c; qb += kU * stride) {
         uint2 e[kU];
@@ -395,31 +430,47 @@ __global__ void __launch_bounds__(256) k_extend_write(const uint32_t* __restrict
       }
       continue;
     }
-    const uint32_t words = c * out_cols;
-    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
-      // float quotient within one of the exact one (w < 2^18); fix it up
-      uint32_t q = __float2uint_rz(((float)w + 0.5f) * inv_out_cols);
-      if (q * out_cols > w) --q;
-      else if ((q + 1) * out_cols <= w) ++q;
-      const uint32_t col = w - q * out_cols;
-      if (o + q < out_cap) {
-        const uint2 e = __ldg(kt + q);
-        out[(o + q) * out_cols + col] = (col < cols) ? __ldg(in + (row_begin + e.x) * cols + col) : e.y;
+    // wider rows: a warp per output row, lanes over its words; kU rows of
+    // a warp in flight at once
+    for (uint32_t qb = wid; qb < c; qb += kU * nwarps) {
+      uint2 e[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const uint32_t q = qb + u * nwarps;
+        e[u] = (q < c && o + q < out_cap) ? __ldg(kt + q) : make_uint2(0xffffffffu, 0u);
+      }
+      for (uint32_t w0 = 0; w0 < out_cols; w0 += 32) {
+        const uint32_t col = w0 + lane;
+        uint32_t val[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          val[u] = (e[u].x != 0xffffffffu && col < cols) ? __ldg(in + (row_begin + e[u].x) * cols + col) : e[u].y;
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+          if (e[u].x != 0xffffffffu && col < out_cols) out[(o + qb + u * nwarps) * out_cols + col] = val[u];
       }
     }
   }
 }
 
-// Blocks of k_extend_check one SM holds at once (registers and shared memory
-// decide it); asked once per process.
+// Blocks of k_extend_check<ITEMS> one SM holds at once (registers and shared
+// memory decide it); asked once per process.
+template <int ITEMS>
 static uint32_t ext_resident_per_sm() {
   static const uint32_t n = [] {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend_check, kExtBlock, 0) != cudaSuccess || b < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend_check<ITEMS>, kExtBlock, 0) != cudaSuccess || b < 1)
       b = 1;
     return (uint32_t)b;
   }();
   return n;
+}
+
+template <int ITEMS>
+static uint32_t ext_grid() {  // persistent extend blocks: all resident at once
+  const uint32_t per_sm =
+      std::min<uint32_t>(std::max<uint32_t>(1, tuning().ext_blocks_per_sm), ext_resident_per_sm<ITEMS>());
+  return (uint32_t)sm_count() * per_sm;
 }
 
 __global__ void k_gather_u64(const unsigned long long* __restrict__ src, const unsigned long long* __restrict__ idx,
@@ -452,14 +503,19 @@ static Lookback next_lb(Workspace& ws, uint64_t tiles) {
   return lb;
 }
 
-uint64_t join_cands_per_extend_tile() { return kExtTile; }
+uint64_t join_cands_per_extend_tile() { return kMinExtTile; }
+uint64_t join_kept_slack() { return 2ull * kMaxExtTile; }
 
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
-  if (nrows > js.rows || nrows * nb > js.rng_entries || (budget + kExtTile - 1) / kExtTile > js.tiles) {
+  const uint32_t items = ext_items();
+  const uint32_t ext_tile = kExtBlock * items;  // one tile size for the whole step
+  const uint64_t ntiles_max = (budget + ext_tile - 1) / ext_tile;
+  if (nrows > js.rows || nrows * nb > js.rng_entries || ntiles_max > js.tiles ||
+      ntiles_max * ext_tile > js.kept_entries) {
     set_last_error("join step: more rows than the step scratch holds");
     throw CudaError{cudaErrorInvalidValue, "join rows"};
   }
@@ -467,19 +523,25 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   Lookback lb1 = next_lb(ws, ltiles);
   k_locate<<<(uint32_t)ltiles, kLocBlock, 0, ws.stream>>>(in, in_cols, row_begin, nrows, d_back, nb, nbrs_total,
                                                           budget, js.drv, js.rng, js.coff, js.tile_row, js.tiles,
-                                                          d_st, lb1);
+                                                          ext_tile, d_st, lb1);
   GPSM_LAUNCHED();
   // check pass: persistent blocks take tiles from a counter until the
   // admitted candidates run out
-  const uint64_t ntiles_max = (budget + kExtTile - 1) / kExtTile;
   GPSM_CUDA(cudaMemsetAsync(js.tile_cnt, 0, std::max<uint64_t>(ntiles_max, 1) * sizeof(uint32_t), ws.stream));
-  k_extend_check<<<ext_grid(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff,
-                                                           js.tile_row, js.kept, js.tile_cnt, d_st, d_inj, ninj);
+  if (items == 8)
+    k_extend_check<8><<<ext_grid<8>(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng,
+                                                                  js.coff, js.tile_row, js.kept, js.tile_cnt, d_st,
+                                                                  d_inj, ninj);
+  else
+    k_extend_check<4><<<ext_grid<4>(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng,
+                                                                  js.coff, js.tile_row, js.kept, js.tile_cnt, d_st,
+                                                                  d_inj, ninj);
   GPSM_LAUNCHED();
   launch_scan_u32(ws, js.tile_cnt, std::max<uint64_t>(ntiles_max, 1), js.tile_off);
   const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));
   k_extend_write<<<wgrid, 256, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
-                                               (uint32_t)std::max<uint64_t>(ntiles_max, 1), out, out_cap, d_st);
+                                               (uint32_t)std::max<uint64_t>(ntiles_max, 1), ext_tile, out, out_cap,
+                                               d_st);
   GPSM_LAUNCHED();
 }
 

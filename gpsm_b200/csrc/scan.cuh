@@ -42,15 +42,17 @@ __device__ __forceinline__ uint32_t lb_take_ticket(const Lookback& lb) {
 }
 
 // Called by all 32 lanes of ONE warp. Publishes `aggregate` for `tile` and
-// returns the exclusive prefix of all earlier tiles (same value in every lane).
+// returns the exclusive prefix of the earlier tiles of its segment (same
+// value in every lane). A segment is a run of tiles scanned on its own:
+// tiles seg_first .. tile-1 are summed; the default is one segment.
 __device__ __forceinline__ unsigned long long lb_exclusive(const Lookback& lb, uint32_t tile,
-                                                           unsigned long long aggregate) {
+                                                           unsigned long long aggregate, uint32_t seg_first = 0) {
   const unsigned lane = threadIdx.x & 31;
   volatile unsigned long long* st = lb.status;
-  if (tile == 0) {
+  if (tile == seg_first) {
     if (lane == 0) {
       __threadfence();
-      st[0] = lb_word(lb.epoch, 2, aggregate);
+      st[tile] = lb_word(lb.epoch, 2, aggregate);
     }
     __syncwarp();
     return 0;
@@ -67,9 +69,9 @@ __device__ __forceinline__ unsigned long long lb_exclusive(const Lookback& lb, u
   while (window_end >= 0) {
     long long idx = window_end - (long long)lane;
     unsigned long long w = 0;
-    uint32_t flag = 2, ep = lb.epoch;  // out-of-range lanes look like a zero prefix
+    uint32_t flag = 2, ep = lb.epoch;  // lanes before the segment look like a zero prefix
     unsigned long long val = 0;
-    if (idx >= 0) {
+    if (idx >= (long long)seg_first) {
       for (;;) {
         w = st[idx];
         ep = (uint32_t)(w >> 44);
@@ -92,6 +94,7 @@ __device__ __forceinline__ unsigned long long lb_exclusive(const Lookback& lb, u
     exclusive += part;
     if (inc) break;
     window_end -= 32;
+    if (window_end < (long long)seg_first) break;
   }
   if (__any_sync(0xffffffffu, timed_out) && lane == 0) atomicOr(lb.flags, (uint32_t)DF_SCAN_TIMEOUT);
   if (lane == 0) {

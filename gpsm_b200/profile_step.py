@@ -1,8 +1,8 @@
 """One batch of a workload on the calling thread, for profilers.
 
     python -m gpsm_b200.profile_step [--workload rmat20] [--first 0] [--count 0]
-                                     [--order learned|plain] [--cap 10000000]
-                                     [--passes 1]
+                                     [--queries 0,2,3] [--order learned|plain]
+                                     [--cap 10000000] [--work-cap 0] [--passes 1]
 
 The bench's timed step runs its queries on engine slots (one host thread
 and one stream each). This driver runs the same queries, order and cap
@@ -27,18 +27,24 @@ def main():
     ap.add_argument("--order", default="learned", choices=["learned", "plain"])
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--passes", type=int, default=1)
+    ap.add_argument("--queries", default="", help="comma-separated batch indices (instead of --first/--count)")
+    ap.add_argument("--work-cap", type=int, default=0, help="candidates a query's joins may scan (0 = none)")
     args = ap.parse_args()
     init(0)
     wl = W.workload(args.workload)
-    qs = wl.queries[args.first:]
-    if args.count:
-        qs = qs[: args.count]
+    if args.queries:
+        qs = [wl.queries[int(i)] for i in args.queries.split(",")]
+    else:
+        qs = wl.queries[args.first:]
+        if args.count:
+            qs = qs[: args.count]
     dg = DeviceGraph(wl.graph)
     model = L.load(0) if args.order == "learned" else None
     packed = pack_queries(qs)
     for p in range(args.passes):
         counts, capped, qms, info = match_batch(dg, qs, cap=args.cap, packed=packed, slots=1,
-                                                orders="learned" if model else None, model=model)
+                                                orders="learned" if model else None, model=model,
+                                                work_cap=args.work_cap)
         print(json.dumps({"pass": p, "queries": len(qs), "device_ms": info["device_ms"], "launches": info["launches"],
                           "expand_launches": info["expand_launches"], "alg_bytes_join": info["alg_bytes_join"],
                           "expand_ms": info["expand_ms"], "rows": int(counts.sum())}), flush=True)

@@ -137,7 +137,8 @@ typedef struct gpsm_match_opts {
   uint32_t pad2;
   gpsm_model_t model;    /* GPSM_ORDER_LEARNED */
   uint64_t memory_budget; /* bytes: predicted peak table above it -> plain order (0 = workspace size) */
-  uint64_t work_cap;     /* candidates the joins may scan before the query stops (0 = none) */
+  uint64_t work_cap;     /* candidates the joins may scan before the query stops, over all of its
+                            join attempts together (a learned plan racing the plain order); 0 = none */
   const uint32_t* edge_labels; /* GPSM_F_DIRECTED: label per query edge (NULL = 1) */
 } gpsm_match_opts;
 
@@ -262,6 +263,13 @@ int gpsm_server_submit(gpsm_server_t s, uint32_t qn, const uint32_t* q_labels, u
                        const uint32_t* q_edges, uint64_t* ticket);
 int gpsm_server_wait(gpsm_server_t s, uint64_t ticket, double timeout_s, gpsm_request_info* info,
                      uint32_t** rows, int32_t* id_map);
+/* The first finished request not yet collected (completion order): its
+ * ticket, info, rows and id_map (room for 128 entries: query vertices are
+ * fewer than 128). A client that takes results as they finish keeps only
+ * unfinished requests' rows in host memory. GPSM_ERR_STATE when nothing is
+ * outstanding; GPSM_ERR_TIMEOUT after timeout_s (< 0: wait). */
+int gpsm_server_wait_any(gpsm_server_t s, double timeout_s, uint64_t* ticket, gpsm_request_info* info,
+                         uint32_t** rows, int32_t* id_map);
 int gpsm_server_stats(gpsm_server_t s, uint64_t* in_use, uint64_t* peak_in_use, uint64_t* budget,
                       uint32_t* queued, uint32_t* active);
 int gpsm_server_destroy(gpsm_server_t s);
@@ -298,6 +306,8 @@ typedef struct gpsm_tuning {
                                   (default 2^22; ~a second at most) */
   uint64_t race_share;         /* learned order: first work share (candidates) when the learned plan
                                   and the plain order take turns (default 2^28) */
+  uint32_t ext_items;          /* candidates per thread of the join check kernel: 4 or 8 (default 4) */
+  uint32_t pad;
 } gpsm_tuning;
 int gpsm_set_tuning(const gpsm_tuning* t);
 int gpsm_get_tuning(gpsm_tuning* t);

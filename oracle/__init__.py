@@ -20,7 +20,9 @@ REF_DISCONNECTED, REF_NO_EDGES, REF_EMPTY_CEDGE = 4, 5, 6
 vp, u32, u64, i32, i64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
 _SIG = {
     "oracle_enumerate": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, u64, vp, u64]),
-    "oracle_enumerate_ordered": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, vp, vp]),
+    "oracle_enumerate_ordered": (i64, [u32, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, vp, vp, vp]),
+    "oracle_label_index": (vp, [u32, vp, vp, vp, C.c_int]),
+    "oracle_label_index_free": (None, [vp]),
     "oracle_ref_plan": (vp, [u32, vp, vp, vp, u32, vp, u32, vp, vp]),
     "oracle_ref_free": (None, [vp]),
     "oracle_ref_info": (None, [vp, vp, vp, vp, vp]),
@@ -163,6 +165,29 @@ def enumerate_embeddings(g, q, cap=1 << 62, rows=True, out_cap=None):
     return None, cnt
 
 
+class _LabelIndex:
+    """Handle of the oracle's label-run index of one graph (freed with it)."""
+
+    def __init__(self, g):
+        self.lib = load()
+        self.g = g  # keeps the CSR arrays alive
+        self.h = self.lib.oracle_label_index(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), os.cpu_count() or 1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_label_index_free(self.h)
+            self.h = None
+
+
+def label_index(g):
+    """The oracle's label-run index of g, built once and kept on g."""
+    li = getattr(g, "_oracle_label_index", None)
+    if li is None:
+        li = _LabelIndex(g)
+        g._oracle_label_index = li
+    return li
+
+
 class WorkBoundHit(Exception):
     """The oracle's search visited its work bound before finishing."""
 
@@ -184,7 +209,7 @@ def enumerate_ordered(g, q, pos2id, cap=1 << 62, work_cap=0, rows=True, with_dig
     dig = u64(0)
     cnt = lib.oracle_enumerate_ordered(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
                                        q.m, _p(qe), _p(order), cap, _p(out), out_cap, work_cap, C.byref(partial),
-                                       C.byref(dig))
+                                       C.byref(dig), label_index(g).h)
     if cnt == -2:
         raise ValueError("pos2id is not a permutation of the query vertices")
     if cnt == -1:

@@ -45,6 +45,70 @@ struct DataGraph {
   }
 };
 
+// Every adjacency list again, ordered by (neighbour label, id), with a
+// directory of label runs per vertex: lets the ordered search scan only the
+// neighbours that carry the next query vertex's label. Built here on host
+// threads, apart from the engine's own (device-built) label runs.
+struct LabelIndex {
+  uint32_t n = 0;
+  const uint32_t* off = nullptr;  // the graph's CSR offsets (lcol uses the same segments)
+  std::vector<uint32_t> lcol;
+  std::vector<uint64_t> run_off;  // [n+1] runs of vertex x: run_off[x] .. run_off[x+1]-1
+  std::vector<uint32_t> run_lab, run_beg;  // label and first lcol index of each run
+  // [b, e) of lcol: x's neighbours with label l (empty when none)
+  void run_of(uint32_t x, uint32_t l, uint32_t* b, uint32_t* e) const {
+    const uint32_t* lo = run_lab.data() + run_off[x];
+    const uint32_t* hi = run_lab.data() + run_off[x + 1];
+    const uint32_t* it = std::lower_bound(lo, hi, l);
+    if (it == hi || *it != l) {
+      *b = *e = 0;
+      return;
+    }
+    const uint64_t k = (uint64_t)(it - run_lab.data());
+    *b = run_beg[k];
+    *e = k + 1 < run_off[x + 1] ? run_beg[k + 1] : off[x + 1];
+  }
+};
+
+static void build_label_index(LabelIndex& L, uint32_t n, const uint32_t* off, const uint32_t* col,
+                              const uint32_t* lab, int threads) {
+  L.n = n;
+  L.off = off;
+  L.lcol.assign(col, col + off[n]);
+  std::vector<uint64_t> runs(n, 0);
+  auto sort_part = [&](uint32_t a, uint32_t b) {
+    for (uint32_t x = a; x < b; ++x) {
+      uint32_t* p = L.lcol.data() + off[x];
+      uint32_t* q = L.lcol.data() + off[x + 1];
+      std::stable_sort(p, q, [&](uint32_t u, uint32_t v) { return lab[u] < lab[v]; });  // ids stay ascending
+      uint64_t r = 0;
+      for (uint32_t* t = p; t < q; ++t) r += (t == p || lab[*t] != lab[t[-1]]);
+      runs[x] = r;
+    }
+  };
+  if (threads < 1) threads = 1;
+  std::vector<std::thread> ts;
+  const uint32_t chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const uint32_t a = std::min<uint64_t>((uint64_t)t * chunk, n), b = std::min<uint64_t>((uint64_t)a + chunk, n);
+    if (a < b) ts.emplace_back(sort_part, a, b);
+  }
+  for (auto& th : ts) th.join();
+  L.run_off.assign(n + 1, 0);
+  for (uint32_t x = 0; x < n; ++x) L.run_off[x + 1] = L.run_off[x] + runs[x];
+  L.run_lab.resize(L.run_off[n]);
+  L.run_beg.resize(L.run_off[n]);
+  for (uint32_t x = 0; x < n; ++x) {
+    uint64_t k = L.run_off[x];
+    for (uint32_t i = off[x]; i < off[x + 1]; ++i)
+      if (i == off[x] || lab[L.lcol[i]] != lab[L.lcol[i - 1]]) {
+        L.run_lab[k] = lab[L.lcol[i]];
+        L.run_beg[k] = i;
+        ++k;
+      }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // 1. independent backtracking oracle
 // ---------------------------------------------------------------------------
@@ -91,6 +155,44 @@ struct Enumerator {
   uint64_t work = 0, work_cap = ~0ULL;  // nodes and candidates visited; optional bound
   bool out_by_pos = false;              // write rows in order position, not by query vertex
   uint64_t digest = 0;                  // rows_digest of the rows found, in order (by position)
+  const LabelIndex* lidx = nullptr;     // optional: scan label runs instead of whole lists
+  // with lidx: arc-consistent candidate sets, one bitset per query vertex
+  std::vector<std::vector<uint64_t>> cand;
+
+  bool in_cand(uint32_t u, uint32_t y) const { return (cand[u][y >> 6] >> (y & 63)) & 1u; }
+
+  // Candidate sets by arc consistency, written from the definition of an
+  // embedding: x stays a candidate of u only while, for every query
+  // neighbour w of u, x has a neighbour that is a candidate of w. An
+  // embedding maps every vertex to a vertex that passes this test forever,
+  // so no embedding is lost; rounds repeat until nothing changes.
+  void filter_candidates() {
+    const size_t words = (g.n + 63) / 64;
+    cand.assign(qn, std::vector<uint64_t>(words, 0));
+    for (uint32_t u = 0; u < qn; ++u)
+      for (uint32_t x = 0; x < g.n; ++x)
+        if (g.lab[x] == qlab[u] && g.deg(x) >= qdeg[u]) cand[u][x >> 6] |= 1ull << (x & 63);
+    const uint32_t* L = lidx->lcol.data();
+    for (bool changed = true; changed;) {
+      changed = false;
+      for (uint32_t u = 0; u < qn; ++u)
+        for (size_t wd = 0; wd < words; ++wd)
+          for (uint64_t bits = cand[u][wd]; bits; bits &= bits - 1) {
+            const uint32_t x = (uint32_t)(wd * 64 + __builtin_ctzll(bits));
+            for (uint32_t w : qadj[u]) {
+              uint32_t b, e;
+              lidx->run_of(x, qlab[w], &b, &e);
+              bool any = false;
+              for (uint32_t i = b; i < e && !any; ++i) any = in_cand(w, L[i]);
+              if (!any) {
+                cand[u][wd] &= ~(1ull << (x & 63));
+                changed = true;
+                break;
+              }
+            }
+          }
+    }
+  }
 
   void make_order() {
     if (!given.empty()) {
@@ -180,12 +282,16 @@ struct Enumerator {
           cap = count;
           return;
         }
-        if (!fits(pos, y)) continue;
+        if (lidx ? !in_cand(u, y) : !fits(pos, y)) continue;
         f[u] = y;
         used[y] = 1;
         dfs(pos + 1);
         used[y] = 0;
       }
+      return;
+    }
+    if (lidx) {
+      dfs_runs(pos, u);
       return;
     }
     // scan the smallest adjacency among mapped neighbours
@@ -211,9 +317,43 @@ struct Enumerator {
     }
   }
 
+  // dfs step with the label index: the shortest label run among the placed
+  // neighbours drives (ascending ids), the others are binary-searched.
+  void dfs_runs(uint32_t pos, uint32_t u) {
+    const auto& bk = back[pos];
+    const size_t nb = bk.size();
+    uint32_t rb[128], re[128];  // query vertices < 128
+    size_t d = 0;
+    for (size_t k = 0; k < nb; ++k) {
+      lidx->run_of(f[bk[k]], qlab[u], &rb[k], &re[k]);
+      if (re[k] - rb[k] < re[d] - rb[d]) d = k;
+    }
+    const uint32_t* L = lidx->lcol.data();
+    uint32_t prev = 0xffffffffu;
+    for (uint32_t i = rb[d]; i < re[d] && count < cap; ++i) {
+      if (++work > work_cap) {
+        cap = count;
+        return;
+      }
+      const uint32_t y = L[i];
+      if (y == prev) continue;  // parallel data edges give one embedding
+      prev = y;
+      if (!in_cand(u, y) || used[y]) continue;
+      bool ok = true;
+      for (size_t k = 0; ok && k < nb; ++k)
+        if (k != d) ok = std::binary_search(L + rb[k], L + re[k], y);
+      if (!ok) continue;
+      f[u] = y;
+      used[y] = 1;
+      dfs(pos + 1);
+      used[y] = 0;
+    }
+  }
+
   void run() {
     if (qn == 0) return;
     make_order();
+    if (lidx) filter_candidates();
     f.assign(qn, 0);
     used.assign(g.n, 0);
     dfs(0);
@@ -679,12 +819,14 @@ int64_t oracle_enumerate(uint32_t n, const uint32_t* off, const uint32_t* col, c
 // (i + 1) * hash(row i), mod 2^64). Returns the count (at most cap), or -1
 // when work_cap search steps (nodes and candidates examined) came first (0 = no bound); then
 // *partial gets the rows found so far.
+// lidx: a handle from oracle_label_index (or NULL: scan whole lists).
 int64_t oracle_enumerate_ordered(uint32_t n, const uint32_t* off, const uint32_t* col, const uint32_t* lab,
                                  uint32_t qn, const uint32_t* qlab, uint32_t qm, const uint32_t* qe,
                                  const int32_t* pos2id, uint64_t cap, uint32_t* out, uint64_t out_cap,
-                                 uint64_t work_cap, uint64_t* partial, uint64_t* digest) {
+                                 uint64_t work_cap, uint64_t* partial, uint64_t* digest, const void* lidx) {
   DataGraph g{n, off, col, lab};
   Enumerator en(g, qn, qlab, qm, qe, cap, out, out_cap);
+  en.lidx = (const LabelIndex*)lidx;
   std::vector<uint8_t> seen(qn, 0);
   for (uint32_t p = 0; p < qn; ++p) {
     const int32_t u = pos2id[p];
@@ -700,6 +842,16 @@ int64_t oracle_enumerate_ordered(uint32_t n, const uint32_t* off, const uint32_t
   if (en.work > en.work_cap) return -1;
   return (int64_t)en.count;
 }
+
+// The label-run index of a graph for oracle_enumerate_ordered (the graph's
+// arrays must outlive it); free with oracle_label_index_free.
+void* oracle_label_index(uint32_t n, const uint32_t* off, const uint32_t* col, const uint32_t* lab, int threads) {
+  LabelIndex* L = new LabelIndex();
+  build_label_index(*L, n, off, col, lab, threads);
+  return L;
+}
+
+void oracle_label_index_free(void* h) { delete (LabelIndex*)h; }
 
 // ---- restatement of the reference pipeline --------------------------------
 // Runs edge list, spanning order, init, refinement, candidate edges (both

@@ -74,3 +74,29 @@ def test_failed_request_reports_the_engine_error(gpu, mixed):
     with pytest.raises(gpu.GpsmError):
         srv.wait(srv.submit(bad))
     srv.close()
+
+
+def test_wait_any_returns_every_request_once_in_completion_order(gpu, mixed):
+    """Results taken as they finish: every ticket comes back exactly once,
+    with the rows of its own query; a request already collected by wait()
+    is not returned again; nothing outstanding is an error, not a hang."""
+    g, qs, dg = mixed
+    srv = gpu.Server(dg, slots=4, cap=200000, collect_rows=True)
+    tickets = {srv.submit(q)[0]: q for q in qs}
+    first = next(iter(tickets))
+    direct = srv.wait((first, tickets[first].n))
+    seen = {first}
+    ends = []
+    for _ in range(len(qs) - 1):
+        (tid, qn), r = srv.wait_any()
+        assert tid in tickets and tid not in seen and qn == tickets[tid].n
+        seen.add(tid)
+        ends.append(r["end_ms"])
+        ref = gpu.match(dg, tickets[tid], cap=200000)
+        assert r["rows"] == ref.count
+        assert np.array_equal(r["table"][:, r["id_map"]], ref.embeddings())
+    assert seen == set(tickets) and direct["status"] == 0
+    assert ends == sorted(ends)  # completion order
+    with pytest.raises(gpu.GpsmError):
+        srv.wait_any(timeout=0.0)
+    srv.close()

@@ -1,16 +1,22 @@
 """Autotuner for the engine's launch choices.
 
-    python -m gpsm_b200.autotune [--workload rmat20] [--queries 24] [--out gpsm_b200/data/tuning.json]
+    python -m gpsm_b200.autotune [--workload rmat22] [--queries 24] [--out gpsm_b200/data/tuning.json]
 
 Times a sample of the workload's queries in the learned join order (device
 time of the whole batch, best of two runs after a warm-up) under every
 combination of:
   heavy_degree       candidates above it get a block each (filter kernels)
   ext_blocks_per_sm  persistent join-check blocks per SM (at most what the
-                     SM holds: 6 at 38 registers a thread)
+                     SM holds for the kernel's register count)
+  ext_items          candidates per thread of the join-check kernel (4 or 8:
+                     its tile is 256 x ext_items candidates; a thread keeps
+                     one row's state and list positions across its items)
   step_cands         candidates one join step may admit
   slots              engine slots running queries at once
 and writes the fastest combination to --out; gpsm_b200.init() applies it.
+Slot counts are compared one process each (--slots; a process sizes every
+slot pool from the memory left free when the pool is created, so a second
+pool in the same process would get less): the grid keeps one count.
 Queries that blow up in any order are left out of the sample (they measure
 the order, not the launch shapes): the sample keeps queries whose device
 time under the default choices is below --max-ms.
@@ -27,16 +33,18 @@ from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
 from . import learned as L
 from . import workloads as W
 
-GRID = dict(heavy_degree=[256, 1024, 4096], ext_blocks_per_sm=[3, 6], step_cands=[1 << 23, 1 << 25],
-            slots=[2, 4, 8])
+GRID = dict(heavy_degree=[1024, 4096], ext_blocks_per_sm=[3, 6], ext_items=[4, 8],
+            step_cands=[1 << 23, 1 << 25], slots=[8])
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="rmat20")
+    ap.add_argument("--workload", default="rmat22")
+    ap.add_argument("--work-cap", type=int, default=5_000_000_000)
     ap.add_argument("--queries", type=int, default=24)
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--max-ms", type=float, default=200.0)
+    ap.add_argument("--slots", type=int, default=0, help="the slot count to tune at (0 = the grid's)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
                                                   "tuning.json"))
     args = ap.parse_args()
@@ -52,13 +60,16 @@ def main():
             sample.append(q)
         if len(sample) >= args.queries:
             break
+    if args.slots:
+        GRID["slots"] = [args.slots]
     results = []
     keys = list(GRID)
     for combo in itertools.product(*[GRID[k] for k in keys]):
         choice = dict(zip(keys, combo))
         set_tuning(**choice)
         def run():
-            return match_batch(dg, sample, cap=args.cap, slots=choice["slots"], orders="learned", model=model)
+            return match_batch(dg, sample, cap=args.cap, slots=choice["slots"], orders="learned", model=model,
+                               work_cap=args.work_cap)
 
         run()  # warm-up
         best = min(run()[3]["device_ms"] for _ in range(2))

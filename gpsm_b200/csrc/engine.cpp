@@ -671,6 +671,11 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   uint32_t* nbrs = C.F.nbrs;
   const uint64_t nbrs_total = C.F.nbrs_total;
   auto bm_of = [&](uint32_t u) { return C.F.bm + (size_t)u * W; };
+  // whatever path leaves this attempt, its row copies to the host have ended
+  struct CopiesDone {
+    Workspace& w;
+    ~CopiesDone() { cudaStreamSynchronize(w.copy_stream); }
+  } copies_done{ws};
   hit_limit = false;
   ws.arena.used = join_mark;
   R.pos2id = pos2id;
@@ -729,7 +734,10 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   }
   uint32_t* d_inj = arena_alloc<uint32_t>(ws, inj.size() + 1);
   if (!inj.empty()) GPSM_CUDA(cudaMemcpyAsync(d_inj, inj.data(), inj.size() * 4, cudaMemcpyHostToDevice, s));
-  StepState* d_st = arena_alloc<StepState>(ws, 1);
+  // two step states used in turn: each step's write pass clears the next
+  // step's one (after the host has read it), so no memset per step
+  StepState* d_st2 = arena_alloc<StepState>(ws, 2);
+  uint32_t st_turn = 0;
   StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
   JoinScratch js;
   uint32_t max_nb = 1;
@@ -746,6 +754,9 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   js.kept = arena_alloc<uint2>(ws, js.kept_entries);
   js.tile_cnt = arena_alloc<uint32_t>(ws, js.tiles);
   js.tile_off = arena_alloc<unsigned long long>(ws, js.tiles + 1);
+  // zero once: every write pass clears the tile counts it read
+  GPSM_CUDA(cudaMemsetAsync(js.tile_cnt, 0, js.tiles * sizeof(uint32_t), s));
+  GPSM_CUDA(cudaMemsetAsync(d_st2, 0, 2 * sizeof(StepState), s));
   GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
 
   R.stats.level_rows.assign(qn + 1, 0);
@@ -770,6 +781,12 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
   if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
   uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
+  // rows bound for a page-locked block get a second result buffer: the
+  // joins fill one while the other is copied out on the copy stream
+  uint32_t* res_bufs[2] = {res_buf, nullptr};
+  int res_cur = 0;
+  if (opt.collect_rows && !opt.keep_on_device && R.host_rows.pinned())
+    res_bufs[1] = (uint32_t*)ws.arena.alloc(std::max<uint64_t>(res_cap * qn, 1) * sizeof(uint32_t));
   // directed mode: final rows land in a staging buffer and only those whose
   // query edges are directed, labelled data edges move to the result
   uint32_t* stage = nullptr;
@@ -804,8 +821,20 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
       res_used = 0;
       return;
     }
-    R.host_rows.append_from_device(ws, res_buf, res_used * qn);
+    const uint64_t words = res_used * qn;
     res_used = 0;
+    if (res_bufs[1]) {
+      GPSM_CUDA(cudaEventRecord(ws.ev_res[res_cur], s));
+      if (R.host_rows.append_from_device_async(ws, res_buf, words, ws.ev_res[res_cur], ws.ev_copied[res_cur])) {
+        res_cur ^= 1;
+        res_buf = res_bufs[res_cur];
+        // the other buffer's earlier copy ends before new rows land in it
+        GPSM_CUDA(cudaStreamWaitEvent(s, ws.ev_copied[res_cur], 0));
+        return;
+      }
+      GPSM_CUDA(cudaStreamSynchronize(ws.copy_stream));  // no copy may be pending into a block that moves
+    }
+    R.host_rows.append_from_device(ws, res_buf, words);
   };
 
   if (qn == 1) {
@@ -886,10 +915,12 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     uint64_t want = (uint64_t)(1.25 * (double)budget / std::max(A.ratio, 1.0 / 1024.0)) + 256;
     want = std::min<uint64_t>(want, js.rows);
     const uint64_t rb = A.next, re = std::min<uint64_t>(A.nrows, A.next + want);
-    GPSM_CUDA(cudaMemsetAsync(d_st, 0, sizeof(StepState), s));
+    StepState* d_st = d_st2 + st_turn;
+    StepState* d_next = d_st2 + (st_turn ^ 1);
+    st_turn ^= 1;
     GPSM_CUDA(cudaEventRecord(ws.eve0, s));
     launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                     out_cap, js, d_st, d_inj + inj_off[lv], inj_cnt[lv]);
+                     out_cap, js, d_st, d_next, d_inj + inj_off[lv], inj_cnt[lv]);
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 4;  // locate, check, scan, write
     ++R.stats.join_steps;

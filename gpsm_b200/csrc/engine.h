@@ -123,6 +123,7 @@ class HostRows {
   HostRows& operator=(HostRows&& o) noexcept;
   ~HostRows();
   uint64_t size() const { return n_; }  // words
+  bool pinned() const { return pinned_; }
   bool empty() const { return n_ == 0; }
   const uint32_t* data() const { return p_; }
   void clear() { n_ = 0; }
@@ -133,6 +134,11 @@ class HostRows {
   uint32_t* append(uint64_t words);
   // append `words` words copied from device memory on ws's stream
   void append_from_device(Workspace& ws, const uint32_t* d_src, uint64_t words);
+  // the same on ws.copy_stream after `ready` (recorded on ws.stream), with
+  // `done` recorded when the copy ends; only into a page-locked block that
+  // already has room (returns false otherwise, and copies nothing)
+  bool append_from_device_async(Workspace& ws, const uint32_t* d_src, uint64_t words, cudaEvent_t ready,
+                                cudaEvent_t done);
   uint32_t* release() {
     uint32_t* q = p_;
     p_ = nullptr, n_ = cap_ = 0, pinned_ = false;

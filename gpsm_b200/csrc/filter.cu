@@ -227,7 +227,7 @@ __device__ __forceinline__ const uint32_t* scan_range_block(const GraphView& g, 
 // Candidates of u are read from C(u)'s bitmap (no compaction before each
 // step): warps of the first `light_blocks` blocks take chunks of `cw` words
 // (1..32, so that small bitmaps still spread over thousands of warps) and
-// handle their candidates one at a time with lanes over
+// handle their candidates four at a time, 8 lanes each over the candidate's
 // neighbours; a candidate with more than `hub_degree` neighbours (a hub) is
 // left to the remaining blocks of the same launch, which walk the hubs of
 // u's label (a prefix of lab_vtx, degree descending) with threads over
@@ -238,23 +238,85 @@ struct StepTargets {
   uint32_t ntgt;
 };
 
-// Explore one candidate mu of u, cooperatively over `group` threads
-// (a warp or a block): every neighbour mv with the target's label and
-// degree >= the target's enters C(v); mu leaves C(u) at the first target
-// that gets none (match/Match.cu:594-598) and later targets are skipped.
-template <bool BLOCK>
+// Label run of mu for label l found by a team of G lanes of one warp (the
+// lanes first .. first+G-1): G directory entries a step; labels ascend in
+// the directory, so the search stops at the first larger label.
+template <int G>
+__device__ __forceinline__ void label_run_team(const GraphView& g, uint32_t mu, uint32_t l, uint32_t end,
+                                               uint32_t* rb, uint32_t* re) {
+  const uint32_t lane = threadIdx.x & 31, first = lane & ~(uint32_t)(G - 1), tl = lane - first;
+  const uint32_t mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << first);
+  const uint32_t db = g.run_off[mu], de = g.run_off[mu + 1];
+  *rb = *re = 0;
+  for (uint32_t k0 = db; k0 < de; k0 += G) {
+    const uint32_t k = k0 + tl;
+    uint2 r = make_uint2(0u, 0u);
+    if (k < de) r = g.runs[k];
+    const uint32_t hit = __ballot_sync(mask, k < de && r.x == l) & mask;
+    if (hit) {
+      const uint32_t src = __ffs(hit) - 1;  // lane holding the run
+      const uint32_t kk = k0 + (src - first);
+      *rb = __shfl_sync(mask, r.y, src);
+      *re = kk + 1 < de ? g.runs[kk + 1].y : end;
+      return;
+    }
+    if (__ballot_sync(mask, k < de && r.x > l) & mask) return;  // l is absent
+  }
+}
+
+// Scan range of mu for label l for a team of G lanes (G = 0: a whole block,
+// each warp looking the run up itself).
+template <int G>
+__device__ __forceinline__ const uint32_t* scan_range_team(const GraphView& g, uint32_t mu, uint32_t l, uint32_t b,
+                                                           uint32_t e, uint32_t* rb, uint32_t* re) {
+  if (g.lcol && e - b > kRunMinDegree) {
+    label_run_team<G == 0 ? 32 : G>(g, mu, l, e, rb, re);
+    return g.lcol;
+  }
+  *rb = b;
+  *re = e;
+  return g.col;
+}
+
+// The threads that work on one candidate: G lanes of a warp, or (G = 0) the
+// whole block; any() is true on every member when it is on one.
+template <int G>
+struct Team {
+  uint32_t rank, size, mask;
+  __device__ __forceinline__ Team() {
+    if (G == 0) {
+      rank = threadIdx.x;
+      size = blockDim.x;
+      mask = 0;
+    } else {
+      const uint32_t lane = threadIdx.x & 31, first = lane & ~(uint32_t)(G - 1);
+      rank = lane - first;
+      size = G;
+      mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << first);
+    }
+  }
+  __device__ __forceinline__ bool any(bool p) const {
+    if (G == 0) return __syncthreads_or(p);
+    return (__ballot_sync(mask, p) & mask) != 0;
+  }
+};
+
+// Explore one candidate mu of u with team T: every neighbour mv with the
+// target's label and degree >= the target's enters C(v); mu leaves C(u) at
+// the first target that gets none (match/Match.cu:594-598) and later
+// targets are skipped.
+template <int G>
 __device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
                                             const uint32_t* s_tgt, uint32_t ntgt, uint32_t* __restrict__ bm,
                                             uint32_t words, uint32_t* bmu) {
-  const uint32_t tid = BLOCK ? threadIdx.x : (threadIdx.x & 31);
-  const uint32_t nthr = BLOCK ? blockDim.x : 32;
+  const Team<G> T;
   for (uint32_t t = 0; t < ntgt; ++t) {
     const uint32_t v = s_tgt[3 * t], lv = s_tgt[3 * t + 1], dv = s_tgt[3 * t + 2];
     uint32_t* bmv = bm + (size_t)v * words;
     bool any = false;
     uint32_t rb, re;
-    const uint32_t* cl = scan_range_warp(g, mu, lv, b, e, &rb, &re);
-    for (uint32_t j = rb + tid; j < re; j += nthr) {
+    const uint32_t* cl = scan_range_team<G>(g, mu, lv, b, e, &rb, &re);
+    for (uint32_t j = rb + T.rank; j < re; j += T.size) {
       const uint32_t mv = cl[j];
       const uint2 ld = g.labdeg[mv];
       if (ld.x == lv && ld.y >= dv) {
@@ -262,38 +324,36 @@ __device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uin
         any = true;
       }
     }
-    const bool got = BLOCK ? __syncthreads_or(any) : __any_sync(0xffffffffu, any);
-    if (!got) {
-      if (tid == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
+    if (!T.any(any)) {
+      if (T.rank == 0) atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
       return;
     }
   }
 }
 
-// Refine one candidate mu of u over `group` threads: mu stays only if every
-// target x has a candidate among mu's neighbours (match/Match.cu:761-808).
-template <bool BLOCK>
+// Refine one candidate mu of u with team T: mu stays only if every target
+// x has a candidate among mu's neighbours (match/Match.cu:761-808).
+template <int G>
 __device__ __forceinline__ void refine_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
                                            const uint32_t* s_tgt, uint32_t ntgt, const uint32_t* __restrict__ bm,
                                            uint32_t words, uint32_t* bmu, const RefineStamp& rs, uint32_t u) {
-  const uint32_t tid = BLOCK ? threadIdx.x : (threadIdx.x & 31);
-  const uint32_t nthr = BLOCK ? blockDim.x : 32;
+  const Team<G> T;
   for (uint32_t t = 0; t < ntgt; ++t) {
     const uint32_t* bmv = bm + (size_t)s_tgt[2 * t] * words;
     bool found = false;
     uint32_t rb, re;
-    const uint32_t* cl = scan_range_warp(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
-    for (uint32_t j0 = rb; j0 < re && !found; j0 += nthr) {
-      const uint32_t j = j0 + tid;
+    const uint32_t* cl = scan_range_team<G>(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
+    for (uint32_t j0 = rb; j0 < re && !found; j0 += T.size) {
+      const uint32_t j = j0 + T.rank;
       bool hit = false;
       if (j < re) {
         const uint32_t mv = cl[j];
         hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
       }
-      found = BLOCK ? __syncthreads_or(hit) : __any_sync(0xffffffffu, hit);
+      found = T.any(hit);
     }
     if (!found) {
-      if (tid == 0) {
+      if (T.rank == 0) {
         atomicAnd(&bmu[mu >> 5], ~(1u << (mu & 31)));
         if (rs.stamp) rs.stamp[u] = rs.seq;
       }
@@ -320,33 +380,45 @@ __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint3
                                                      uint32_t* __restrict__ bm, uint32_t words,
                                                      const uint32_t* __restrict__ flags, RefineStamp rs) {
   constexpr uint32_t kStride = EXPLORE ? 3 : 2;
+  constexpr uint32_t kTeam = 8;  // lanes per candidate in the light part
   extern __shared__ uint32_t s_tgt[];
+  __shared__ uint32_t s_chunk[8][32 * 32];  // per warp: the candidates of one chunk (at most 32 words)
   for (uint32_t i = threadIdx.x; i < kStride * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
   if (*flags & DF_EMPTY) return;
   if (!EXPLORE && refine_is_noop(rs, s_tgt, ntgt)) return;
   uint32_t* bmu = bm + (size_t)u * words;
   if (blockIdx.x < light_blocks) {
+    // each warp lists its chunk's candidates (ascending) in shared memory,
+    // then its four 8-lane teams take them in turn: four candidates' chains
+    // of dependent loads in flight per warp instead of one
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nwarps = light_blocks * (blockDim.x >> 5);
+    uint32_t* wl = s_chunk[threadIdx.x >> 5];
     for (uint32_t c0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * cw; c0 < words; c0 += nwarps * cw) {
       // each word of the chunk belongs to this warp alone: only its own
       // candidates' bits are cleared while it runs
       const uint32_t wv = (lane < cw && c0 + lane < words) ? bmu[c0 + lane] : 0u;
-      uint32_t pending = __ballot_sync(0xffffffffu, wv != 0);
-      while (pending) {
-        const uint32_t src = __ffs(pending) - 1;
-        pending &= pending - 1;
-        uint32_t word = __shfl_sync(0xffffffffu, wv, src);
-        while (word) {
-          const uint32_t mu = (c0 + src) * 32 + (__ffs(word) - 1);
-          word &= word - 1;
-          const uint32_t b = g.off[mu], e = g.off[mu + 1];
-          if (e - b > hub_degree) continue;  // a hub: the hub blocks take it
-          if (EXPLORE) explore_one<false>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
-          else refine_one<false>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
-        }
+      const uint32_t c = __popc(wv);
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += x;
       }
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      if (total == 0) continue;
+      uint32_t p = incl - c;
+      for (uint32_t x = wv; x; x &= x - 1) wl[p++] = (c0 + lane) * 32 + (__ffs(x) - 1);
+      __syncwarp();
+      for (uint32_t i = lane / kTeam; i < total; i += 32 / kTeam) {
+        const uint32_t mu = wl[i];
+        const uint32_t b = g.off[mu], e = g.off[mu + 1];
+        if (e - b > hub_degree) continue;  // a hub: the hub blocks take it
+        if (EXPLORE) explore_one<kTeam>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
+        else refine_one<kTeam>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
+      }
+      __syncwarp();  // the list is rewritten for the next chunk
     }
     return;
   }
@@ -354,8 +426,8 @@ __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint3
     const uint32_t mu = lab_vtx[i];
     if (!((bmu[mu >> 5] >> (mu & 31)) & 1u)) continue;  // not (or no longer) a candidate of u
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    if (EXPLORE) explore_one<true>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
-    else refine_one<true>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
+    if (EXPLORE) explore_one<0>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu);
+    else refine_one<0>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
     __syncthreads();  // the bitmap word read above is read again for the next hub
   }
 }
@@ -372,30 +444,48 @@ __device__ __forceinline__ uint32_t find_dir(const unsigned long long* __restric
   return lo;
 }
 
+// Defers a hub item to the block kernels (team version of defer_heavy).
+template <int G>
+__device__ __forceinline__ bool defer_heavy_team(const Team<G>& T, uint32_t deg, uint32_t item, HeavyList hl) {
+  if (deg <= hl.threshold || hl.items == nullptr) return false;
+  const uint32_t lead = __ffs(T.mask) - 1;
+  uint32_t slot = 0;
+  if (T.rank == 0) slot = atomicAdd(hl.count, 1u);
+  slot = __shfl_sync(T.mask, slot, lead);
+  if (slot >= hl.cap) return false;  // list full: the team does it
+  if (T.rank == 0) hl.items[slot] = item;
+  return true;
+}
+
+// Candidate-edge work items (edge direction u->v, mu in C(u)) go to teams of
+// kCedgeTeam lanes (four items per warp in flight); hubs go to the block
+// kernels through the deferred list.
+constexpr int kCedgeTeam = 8;
+
 // Per (edge direction u->v, mu in C(u)): |N(mu) ∩ C(v)|.
 __global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir* __restrict__ dirs,
                                                      uint32_t ndir, const unsigned long long* __restrict__ s_base,
                                                      const uint32_t* __restrict__ bm, uint32_t words,
                                                      uint32_t* __restrict__ cnt, HeavyList hl) {
+  const Team<kCedgeTeam> T;
   const unsigned long long items = s_base[ndir];
-  const uint32_t lane = threadIdx.x & 31;
-  const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += warps) {
+  const unsigned long long teams = (gridDim.x * blockDim.x) / kCedgeTeam;
+  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) / kCedgeTeam; w < items; w += teams) {
     const uint32_t d = find_dir(s_base, ndir, w);
     const CedgeDir cd = dirs[d];
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
+    if (defer_heavy_team(T, e - b, (uint32_t)w, hl)) continue;
     uint32_t rb, re;
-    const uint32_t* cl = scan_range_warp(g, mu, cd.lab, b, e, &rb, &re);
+    const uint32_t* cl = scan_range_team<kCedgeTeam>(g, mu, cd.lab, b, e, &rb, &re);
     uint32_t c = 0;
-    for (uint32_t j = rb + lane; j < re; j += 32) {
+    for (uint32_t j = rb + T.rank; j < re; j += kCedgeTeam) {
       const uint32_t mv = cl[j];
       c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
     }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) cnt[w] = c;
+    for (int o = kCedgeTeam / 2; o > 0; o >>= 1) c += __shfl_xor_sync(T.mask, c, o);
+    if (T.rank == 0) cnt[w] = c;
   }
 }
 
@@ -405,29 +495,30 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
                                                      const uint32_t* __restrict__ bm, uint32_t words,
                                                      const unsigned long long* __restrict__ goff,
                                                      uint32_t* __restrict__ nbrs, HeavyList hl) {
+  const Team<kCedgeTeam> T;
+  const uint32_t lead = __ffs(T.mask) - 1;
   const unsigned long long items = s_base[ndir];
-  const uint32_t lane = threadIdx.x & 31;
-  const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += warps) {
+  const unsigned long long teams = (gridDim.x * blockDim.x) / kCedgeTeam;
+  for (unsigned long long w = (blockIdx.x * blockDim.x + threadIdx.x) / kCedgeTeam; w < items; w += teams) {
     const uint32_t d = find_dir(s_base, ndir, w);
     const CedgeDir cd = dirs[d];
     const uint32_t mu = cd.ids[w - cd.item_base];
     const uint32_t* bmv = bm + (size_t)cd.v * words;
     const uint32_t b = g.off[mu], e = g.off[mu + 1];
-    if (defer_heavy(e - b, (uint32_t)w, hl)) continue;
+    if (defer_heavy_team(T, e - b, (uint32_t)w, hl)) continue;
     uint32_t rb, re;
-    const uint32_t* cl = scan_range_warp(g, mu, cd.lab, b, e, &rb, &re);
+    const uint32_t* cl = scan_range_team<kCedgeTeam>(g, mu, cd.lab, b, e, &rb, &re);
     unsigned long long pos = goff[w];
-    for (uint32_t j0 = rb; j0 < re; j0 += 32) {
-      const uint32_t j = j0 + lane;
+    for (uint32_t j0 = rb; j0 < re; j0 += kCedgeTeam) {
+      const uint32_t j = j0 + T.rank;
       uint32_t mv = 0;
       bool hit = false;
       if (j < re) {
         mv = cl[j];
         hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
       }
-      const uint32_t bal = __ballot_sync(0xffffffffu, hit);
-      if (hit) nbrs[pos + __popc(bal & ((1u << lane) - 1))] = mv;
+      const uint32_t bal = (__ballot_sync(T.mask, hit) & T.mask) >> lead;  // bit r: team rank r
+      if (hit) nbrs[pos + __popc(bal & ((1u << T.rank) - 1u))] = mv;
       pos += __popc(bal);
     }
   }
@@ -665,7 +756,7 @@ void launch_cedge_count(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_d
                         const unsigned long long* d_base, uint64_t items, const uint32_t* bm, uint32_t* cnt) {
   if (items == 0) return;
   HeavyList hl = heavy_list(ws, g);
-  uint32_t blocks = grid_for(items, 148 * 16);
+  uint32_t blocks = grid_for((items + 3) / 4, 148 * 16);
   k_cedge_count<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, cnt, hl);
   GPSM_LAUNCHED();
   if (hl.items) {
@@ -679,7 +770,7 @@ void launch_cedge_write(Workspace& ws, const DeviceGraph& g, const CedgeDir* d_d
                         const unsigned long long* goff, uint32_t* nbrs) {
   if (items == 0) return;
   HeavyList hl = heavy_list(ws, g);
-  uint32_t blocks = grid_for(items, 148 * 16);
+  uint32_t blocks = grid_for((items + 3) / 4, 148 * 16);
   k_cedge_write<<<blocks, 256, 0, ws.stream>>>(view(g), d_dirs, ndir, d_base, bm, g.words, goff, nbrs, hl);
   GPSM_LAUNCHED();
   if (hl.items) {

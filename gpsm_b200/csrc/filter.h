@@ -125,6 +125,9 @@ uint64_t join_cands_per_extend_tile();
 uint64_t join_kept_slack();
 
 // One join step over input rows [row_begin, row_end) (in_cols columns,
+// d_st: this step's state, zero on entry; d_next: the next step's, cleared
+// by this step once its last launch no longer reads d_st; js.tile_cnt must
+// be zero on entry and is left zero;
 // row-major): rows are admitted in order while their candidates fit
 // `budget`; admitted rows are extended by the query vertex whose placed
 // neighbours are back[0..nb) into `out` (in_cols+1 columns), at most out_cap
@@ -133,6 +136,7 @@ uint64_t join_kept_slack();
 // label (the only columns a candidate can repeat).
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
-                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj);
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
+                      const uint32_t* d_inj, uint32_t ninj);
 
 }  // namespace gpsm

@@ -302,6 +302,11 @@ Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) 
   ws->device = device;
   try {
     GPSM_CUDA(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    GPSM_CUDA(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      GPSM_CUDA(cudaEventCreateWithFlags(&ws->ev_res[i], cudaEventDisableTiming));
+      GPSM_CUDA(cudaEventCreateWithFlags(&ws->ev_copied[i], cudaEventDisableTiming));
+    }
     GPSM_CUDA(cudaMalloc(&ws->arena.base, arena_bytes));
     ws->arena.size = arena_bytes;
     ws->scan.max_tiles = max_tiles;
@@ -326,6 +331,7 @@ Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) 
   } catch (...) {
     // partial construction: release what exists
     if (ws->stream) cudaStreamDestroy(ws->stream);
+    if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
     cudaFree(ws->arena.base);
     cudaFree(ws->scan.d_ticket);
     cudaFree(ws->scan.d_status);
@@ -344,7 +350,13 @@ void workspace_free(Workspace* ws) {
   if (!ws) return;
   cudaSetDevice(ws->device);
   cudaStreamSynchronize(ws->stream);
+  cudaStreamSynchronize(ws->copy_stream);
   cudaStreamDestroy(ws->stream);
+  cudaStreamDestroy(ws->copy_stream);
+  for (int i = 0; i < 2; ++i) {
+    if (ws->ev_res[i]) cudaEventDestroy(ws->ev_res[i]);
+    if (ws->ev_copied[i]) cudaEventDestroy(ws->ev_copied[i]);
+  }
   cudaFree(ws->arena.base);
   cudaFree(ws->scan.d_ticket);
   cudaFree(ws->scan.d_status);

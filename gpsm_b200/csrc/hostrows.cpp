@@ -180,6 +180,17 @@ void HostRows::append_from_device(Workspace& ws, const uint32_t* d_src, uint64_t
   }
 }
 
+bool HostRows::append_from_device_async(Workspace& ws, const uint32_t* d_src, uint64_t words, cudaEvent_t ready,
+                                        cudaEvent_t done) {
+  if (!pinned_ || n_ + words > cap_ || !ws.copy_stream) return false;
+  if (words == 0) return true;
+  uint32_t* dst = append(words);
+  GPSM_CUDA(cudaStreamWaitEvent(ws.copy_stream, ready, 0));
+  GPSM_CUDA(cudaMemcpyAsync(dst, d_src, words * sizeof(uint32_t), cudaMemcpyDeviceToHost, ws.copy_stream));
+  GPSM_CUDA(cudaEventRecord(done, ws.copy_stream));
+  return true;
+}
+
 void copy_to_host(Workspace& ws, uint32_t* dst, const uint32_t* d_src, uint64_t words) {
   if (words == 0) return;
   cudaStream_t s = ws.stream;

@@ -156,6 +156,11 @@ struct Workspace {
   static constexpr size_t kStageBytes = 32ull << 20;
   void* h_stage[2] = {nullptr, nullptr};
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+  // result rows copied to page-locked host blocks on their own stream, so a
+  // slot's joins fill one device result buffer while the other is copied
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_res[2] = {nullptr, nullptr};     // buffer k written (on stream)
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr};  // buffer k copied out (on copy_stream)
 };
 
 // Copies `words` 32-bit words from device memory to pageable host memory

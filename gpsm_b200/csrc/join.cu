@@ -55,11 +55,13 @@ constexpr int kInjReg = 8;  // injectivity columns a thread holds in registers p
 // Candidates per check thread of the next step (tuning; 4 or 8).
 static uint32_t ext_items() { return tuning().ext_items >= 8 ? 8u : 4u; }
 
-// First index in a[lo, hi) whose value is >= key (hi when none).
-__device__ __forceinline__ unsigned long long lower_bound_u32(const uint32_t* __restrict__ a, unsigned long long lo,
-                                                              unsigned long long hi, uint32_t key) {
+// First index in a[lo, hi) whose value is >= key (hi when none). Indices
+// are 32-bit offsets from the list's base pointer (a list is shorter than
+// 2^32), which keeps each probe to a few integer instructions.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                                    uint32_t key) {
   while (lo < hi) {
-    const unsigned long long mid = (lo + hi) >> 1;
+    const uint32_t mid = (lo + hi) >> 1;
     if (__ldg(a + mid) < key) lo = mid + 1;
     else hi = mid;
   }
@@ -69,9 +71,9 @@ __device__ __forceinline__ unsigned long long lower_bound_u32(const uint32_t* __
 // The same, given that every value before lo is < key: probes lo, lo+1,
 // lo+3, lo+7, ... until a value >= key, then a binary search inside the last
 // gap; O(log d) for an answer d places after lo.
-__device__ __forceinline__ unsigned long long gallop_u32(const uint32_t* __restrict__ a, unsigned long long lo,
-                                                         unsigned long long hi, uint32_t key) {
-  unsigned long long step = 1, probe = lo;
+__device__ __forceinline__ uint32_t gallop_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                               uint32_t key) {
+  uint32_t step = 1, probe = lo;
   while (probe < hi && __ldg(a + probe) < key) {
     lo = probe + 1;
     probe = lo + step;
@@ -336,22 +338,22 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
       }
       // pass 2: y must lie in every other placed neighbour's list
       for (uint32_t j = 0; keep && j < nb; ++j) {
-        const uint32_t* __restrict__ list = S.back[j].nbrs;
         uint32_t cur = 0xffffffffu;
-        unsigned long long pos = 0, hi = 0;
+        const uint32_t* __restrict__ list = nullptr;  // this row's list towards v, from its first entry
+        uint32_t pos = 0, len = 0;
 #pragma unroll
         for (int k = 0; k < ITEMS; ++k) {
           if (!((keep >> k) & 1u) || kd[k] == j) continue;
-          if (kr[k] != cur) {  // first candidate of this row in this list: search the whole range
+          if (kr[k] != cur) {  // first candidate of this row in this list: search the whole list
             cur = kr[k];
             const uint4 g2 = __ldg(rng + (unsigned long long)cur * nb + j);
-            pos = ((unsigned long long)g2.y << 32) | g2.x;
-            hi = pos + g2.z;
-            pos = lower_bound_u32(list, pos, hi, ky[k]);
+            list = S.back[j].nbrs + (((unsigned long long)g2.y << 32) | g2.x);
+            len = g2.z;
+            pos = lower_bound_u32(list, 0, len, ky[k]);
           } else {
-            pos = gallop_u32(list, pos, hi, ky[k]);
+            pos = gallop_u32(list, pos, len, ky[k]);
           }
-          if (!(pos < hi && __ldg(list + pos) == ky[k])) keep &= ~(1u << k);
+          if (!(pos < len && __ldg(list + pos) == ky[k])) keep &= ~(1u << k);
         }
       }
     }
@@ -387,14 +389,16 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
 
 // Block per tile (grid-stride): the tile's kept rows go to output rows
 // tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
-// written. Every load a lane issues for a group of rows is issued before
+// written and clears the next step's state; each tile's count is cleared
+// once read, so the next step's check pass starts from zero counts. Every load a lane issues for a group of rows is issued before
 // its stores, so each lane has kU kept pairs, then kU input words, in flight.
 __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
                                                       unsigned long long row_begin, const uint2* __restrict__ kept,
-                                                      const uint32_t* __restrict__ tile_cnt,
+                                                      uint32_t* __restrict__ tile_cnt,
                                                       const unsigned long long* __restrict__ tile_off,
                                                       uint32_t ntiles_max, uint32_t ext_tile, uint32_t* __restrict__ out,
-                                                      unsigned long long out_cap, StepState* __restrict__ st) {
+                                                      unsigned long long out_cap, StepState* __restrict__ st,
+                                                      StepState* __restrict__ next) {
   constexpr int kU = 8;
   const uint32_t out_cols = cols + 1;
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -402,10 +406,15 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
   const uint32_t rpw = out_cols <= 32 ? 32 / out_cols : 0;
   const uint32_t lane_q = rpw ? lane / out_cols : 0, lane_c = rpw ? lane - lane_q * out_cols : 0;
   const bool lane_on = rpw && lane < rpw * out_cols;
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->written = min(tile_off[ntiles_max], out_cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->written = min(tile_off[ntiles_max], out_cap);
+    *next = StepState{};  // the next step starts from zero
+  }
   for (uint32_t tile = blockIdx.x; tile < ntiles_max; tile += gridDim.x) {
     const uint32_t c = tile_cnt[tile];
     const unsigned long long o = tile_off[tile];
+    __syncthreads();  // every thread has read the count: clear it for the next step
+    if (threadIdx.x == 0 && c) tile_cnt[tile] = 0;
     if (c == 0 || o >= out_cap) continue;
     const uint2* kt = kept + (unsigned long long)tile * ext_tile;
     if (rpw) {
@@ -508,7 +517,8 @@ uint64_t join_kept_slack() { return 2ull * kMaxExtTile; }
 
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
-                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, const uint32_t* d_inj, uint32_t ninj) {
+                      uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
+                      const uint32_t* d_inj, uint32_t ninj) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
   const uint32_t items = ext_items();
@@ -527,7 +537,6 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   GPSM_LAUNCHED();
   // check pass: persistent blocks take tiles from a counter until the
   // admitted candidates run out
-  GPSM_CUDA(cudaMemsetAsync(js.tile_cnt, 0, std::max<uint64_t>(ntiles_max, 1) * sizeof(uint32_t), ws.stream));
   if (items == 8)
     k_extend_check<8><<<ext_grid<8>(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng,
                                                                   js.coff, js.tile_row, js.kept, js.tile_cnt, d_st,
@@ -541,7 +550,7 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));
   k_extend_write<<<wgrid, 256, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
                                                (uint32_t)std::max<uint64_t>(ntiles_max, 1), ext_tile, out, out_cap,
-                                               d_st);
+                                               d_st, d_next);
   GPSM_LAUNCHED();
 }
 

@@ -8,6 +8,7 @@ the product (gpsm_b200, libgpsm.so) never does.
 import ctypes as C
 import os
 import subprocess
+import threading
 
 import numpy as np
 
@@ -179,13 +180,18 @@ class _LabelIndex:
             self.h = None
 
 
+_INDEX_LOCK = threading.Lock()
+
+
 def label_index(g):
-    """The oracle's label-run index of g, built once and kept on g."""
-    li = getattr(g, "_oracle_label_index", None)
-    if li is None:
-        li = _LabelIndex(g)
-        g._oracle_label_index = li
-    return li
+    """The oracle's label-run index of g, built once (by one thread) and
+    kept on g."""
+    with _INDEX_LOCK:
+        li = getattr(g, "_oracle_label_index", None)
+        if li is None:
+            li = _LabelIndex(g)
+            g._oracle_label_index = li
+        return li
 
 
 class WorkBoundHit(Exception):
@@ -207,9 +213,10 @@ def enumerate_ordered(g, q, pos2id, cap=1 << 62, work_cap=0, rows=True, with_dig
     out = np.zeros((max(out_cap, 1), q.n), np.uint32) if rows else None
     partial = u64(0)
     dig = u64(0)
+    li = label_index(g)  # held for the whole call
     cnt = lib.oracle_enumerate_ordered(g.n, _p(g.offsets), _p(g.cols), _p(g.labels), q.n, _p(_u32(q.labels)),
                                        q.m, _p(qe), _p(order), cap, _p(out), out_cap, work_cap, C.byref(partial),
-                                       C.byref(dig), label_index(g).h)
+                                       C.byref(dig), li.h)
     if cnt == -2:
         raise ValueError("pos2id is not a permutation of the query vertices")
     if cnt == -1:

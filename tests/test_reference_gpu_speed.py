@@ -4,7 +4,8 @@ vertices), through the same driver loop (main/run.cpp:70-97): per query,
 Match::match, IO::output (host verify + text), flush; `match used` is the
 loop's wall time. The 10 queries are repeated so that the millisecond timer
 resolves the loop. Both programs must write the same file; the engine must
-be faster. Prints both times and the ratio."""
+be at least 1.5x faster (the target on this configuration). Prints both
+times and the ratio."""
 import os
 import re
 import subprocess
@@ -65,4 +66,4 @@ def test_engine_beats_reference_build_on_small_er(gpu, tmp_path):
     ratio = t_ref / max(t_our, 1)
     print(f"\nsmall ER, {nq} queries: reference build {t_ref} ms ({nq / max(t_ref, 1) * 1e3:.0f} q/s), "
           f"engine {t_our} ms ({nq / max(t_our, 1) * 1e3:.0f} q/s), ratio {ratio:.2f}")
-    assert t_our < t_ref
+    assert ratio >= 1.5, (t_ref, t_our)

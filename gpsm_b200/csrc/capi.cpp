@@ -351,6 +351,7 @@ int gpsm_set_tuning(const gpsm_tuning* t) {
   if (t->race_share) T.race_share = t->race_share;
   if (t->scan_spin_limit) T.scan_spin_limit = t->scan_spin_limit;
   if (t->ext_items) T.ext_items = t->ext_items >= 8 ? 8u : 4u;
+  if (t->filter_team) T.filter_team = t->filter_team >= 32 ? 32u : 8u;
   return GPSM_OK;
 }
 
@@ -365,7 +366,7 @@ int gpsm_get_tuning(gpsm_tuning* t) {
   t->scan_spin_limit = T.scan_spin_limit;
   t->race_share = T.race_share;
   t->ext_items = T.ext_items;
-  t->pad = 0;
+  t->filter_team = T.filter_team;
   return GPSM_OK;
 }
 

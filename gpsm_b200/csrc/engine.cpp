@@ -773,11 +773,24 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   R.stats.level_rows[1] = L[1].nrows;
   const uint64_t min_rows = (uint64_t)g.max_degree + 64;
   const uint64_t lb = level_buffer_bytes(ws, opt, qn);
+  // Levels 2..qn-1 share one stack of the same total size as one buffer per
+  // level. A level is extended only when every deeper level is empty, so
+  // level w+1 can start right after level w's rows, and a step may use the
+  // free top of the stack less a minimum for each deeper level: never less
+  // room than its own buffer would give (fixed_rows), and more as the
+  // attempt's work grows (stack_ramp), so a long query's deep steps are not
+  // held to one level's share while a capped query, which ends early, keeps
+  // the small steps that waste little past its cap.
+  std::vector<uint64_t> fixed_rows(qn + 1, 0), reserve_words(qn + 2, 0);
+  uint64_t stack_words = 0;
   for (uint32_t w = 2; w < qn; ++w) {
-    uint64_t rows = std::max<uint64_t>(lb / (4ull * w), min_rows);
-    L[w].cap_rows = rows;
-    L[w].buf = arena_alloc<uint32_t>(ws, rows * w);
+    fixed_rows[w] = std::max<uint64_t>(lb / (4ull * w), min_rows);
+    stack_words += (fixed_rows[w] * w + 3) & ~3ull;
   }
+  for (uint32_t w = qn - 1; w >= 2; --w) reserve_words[w] = reserve_words[w + 1] + ((min_rows * w + 3) & ~3ull);
+  uint32_t* stack = qn > 2 ? arena_alloc<uint32_t>(ws, stack_words) : nullptr;
+  uint32_t* const stack_end = stack ? stack + stack_words : nullptr;
+  if (qn > 2) L[2].buf = stack;
   uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
   if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
   uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
@@ -904,10 +917,23 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
       }
     } else {
       Level& B = L[lv + 1];
+      const uint32_t wb = (uint32_t)lv + 1;
       B.nrows = 0;
       B.next = 0;
+      if (lv >= 2) B.buf = L[lv].buf + ((L[lv].nrows * (uint64_t)lv + 3) & ~3ull);  // after level lv's rows
+      const uint64_t room = (uint64_t)(stack_end - B.buf);
+      const uint64_t free_rows = room > reserve_words[wb + 1] ? (room - reserve_words[wb + 1]) / wb : 0;
+      // the step's room beyond its own buffer grows with the attempt's work:
+      // one doubling per doubling of the candidates scanned past 2^26
+      uint64_t ramp = fixed_rows[wb];
+      for (uint64_t c = cands_total >> 26; c > 0 && ramp < free_rows; c >>= 1) ramp *= 2;
       out = B.buf;
-      out_cap = B.cap_rows;
+      out_cap = std::min<uint64_t>(free_rows, std::max<uint64_t>(fixed_rows[wb], ramp));
+      if (out_cap < min_rows) {
+        set_last_error("join level stack exhausted");
+        return GPSM_ERR_BUDGET;
+      }
+      B.cap_rows = out_cap;
       budget = std::min<uint64_t>(out_cap, opt.step_cands);
     }
     // rows offered to this step: enough to fill the budget at the observed

@@ -115,6 +115,8 @@ struct Tuning {
   // candidates per thread of the join check kernel (4 or 8): its tile is
   // 256 x ext_items candidates
   uint32_t ext_items = 4;
+  // lanes per candidate in the refinement steps (8 or 32)
+  uint32_t filter_team = 8;
 };
 Tuning& tuning();
 int sm_count();

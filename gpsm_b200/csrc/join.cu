@@ -387,79 +387,107 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
   }
 }
 
+// Bulk copy shared -> global on the async (TMA) engine, in a bulk group.
+// Both addresses and the size must be multiples of 16 bytes: callers check.
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst), "r"(s), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// Waits until at most N bulk groups of this thread still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;\n" ::"n"(N) : "memory");
+}
+// Waits until every bulk group of this thread has completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
+constexpr uint32_t kWriteStage = 4096;  // words per staging buffer (two buffers)
+
 // Block per tile (grid-stride): the tile's kept rows go to output rows
 // tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
 // written and clears the next step's state; each tile's count is cleared
-// once read, so the next step's check pass starts from zero counts. Every load a lane issues for a group of rows is issued before
-// its stores, so each lane has kU kept pairs, then kU input words, in flight.
+// once read, so the next step's check pass starts from zero counts.
+// The tile's output is one contiguous span. It is built in chunks of whole
+// rows in shared memory, one output word per thread at a time (its row by a
+// multiply-high with the precomputed reciprocal of the row width, exact for
+// these ranges; kU words' loads in flight per thread: the kept pair, then
+// the input row's word) and each chunk leaves by one bulk copy on the async
+// engine; the chunk is laid out so that every word has the
+// same 16-byte phase in shared memory as in the output, so the aligned middle
+// goes in one copy and at most three words at each end by plain stores. Two
+// staging buffers alternate: gathering the next chunk overlaps the copy of
+// the previous one.
 __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
-                                                      unsigned long long row_begin, const uint2* __restrict__ kept,
-                                                      uint32_t* __restrict__ tile_cnt,
-                                                      const unsigned long long* __restrict__ tile_off,
-                                                      uint32_t ntiles_max, uint32_t ext_tile, uint32_t* __restrict__ out,
-                                                      unsigned long long out_cap, StepState* __restrict__ st,
-                                                      StepState* __restrict__ next) {
-  constexpr int kU = 8;
+                                                         unsigned long long row_begin, const uint2* __restrict__ kept,
+                                                         uint32_t* __restrict__ tile_cnt,
+                                                         const unsigned long long* __restrict__ tile_off,
+                                                         uint32_t ntiles_max, uint32_t ext_tile, uint32_t* __restrict__ out,
+                                                         unsigned long long out_cap, StepState* __restrict__ st,
+                                                         StepState* __restrict__ next) {
+  constexpr int kU = 4;
+  __shared__ __align__(128) uint32_t sbuf[2][kWriteStage + 4];
   const uint32_t out_cols = cols + 1;
-  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  // rows of at most 32 words: lane -> (row within a group of rpw rows, column)
-  const uint32_t rpw = out_cols <= 32 ? 32 / out_cols : 0;
-  const uint32_t lane_q = rpw ? lane / out_cols : 0, lane_c = rpw ? lane - lane_q * out_cols : 0;
-  const bool lane_on = rpw && lane < rpw * out_cols;
+  const uint32_t chunk_rows = kWriteStage / out_cols;  // >= 31: rows hold at most 128 words
+  // ceil(2^32 / out_cols): __umulhi(k, recip) == k / out_cols for every
+  // k < 2^32 / out_cols (here k < kWriteStage)
+  const uint32_t recip = (uint32_t)((0x100000000ull + out_cols - 1) / out_cols);
+  const uint32_t* __restrict__ inb = in + row_begin * cols;  // row r of this step: inb + r * cols
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->written = min(tile_off[ntiles_max], out_cap);
     *next = StepState{};  // the next step starts from zero
   }
+  uint32_t chunk_no = 0;  // chunks this block has issued (selects the staging buffer)
   for (uint32_t tile = blockIdx.x; tile < ntiles_max; tile += gridDim.x) {
     const uint32_t c = tile_cnt[tile];
     const unsigned long long o = tile_off[tile];
     __syncthreads();  // every thread has read the count: clear it for the next step
     if (threadIdx.x == 0 && c) tile_cnt[tile] = 0;
     if (c == 0 || o >= out_cap) continue;
+    const uint32_t rows = (uint32_t)min((unsigned long long)c, out_cap - o);
     const uint2* kt = kept + (unsigned long long)tile * ext_tile;
-    if (rpw) {
-      // each warp writes rpw whole rows per store (one contiguous span)
-      const uint32_t stride = nwarps * rpw;
-      for (uint32_t qb = wid * rpw; qb < c; qb += kU * stride) {
+    for (uint32_t q0 = 0; q0 < rows; q0 += chunk_rows, ++chunk_no) {
+      const uint32_t nq = min(chunk_rows, rows - q0);
+      const uint32_t words = nq * out_cols;
+      uint32_t* dst = out + (o + q0) * out_cols;
+      const uint32_t lead = (uint32_t)(((uintptr_t)dst >> 2) & 3);  // dst's word phase within 16 bytes
+      uint32_t* sb = sbuf[chunk_no & 1];
+      if (threadIdx.x == 0) bulk_wait_read<1>();  // the copy that last read this buffer is done with it
+      __syncthreads();
+      for (uint32_t kb = threadIdx.x; kb < words; kb += kU * blockDim.x) {
+        uint32_t col[kU], val[kU];
         uint2 e[kU];
-        bool on[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
-          const uint32_t q = qb + u * stride + lane_q;
-          on[u] = lane_on && q < c && o + q < out_cap;
-          e[u] = on[u] ? __ldg(kt + q) : make_uint2(0u, 0u);
+          const uint32_t k = kb + u * blockDim.x;
+          const uint32_t q = __umulhi(k, recip);
+          col[u] = k - q * out_cols;
+          e[u] = k < words ? __ldg(kt + q0 + q) : make_uint2(0u, 0u);
         }
-        uint32_t val[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u)
-          val[u] = (on[u] && lane_c < cols) ? __ldg(in + (row_begin + e[u].x) * cols + lane_c) : e[u].y;
+          val[u] = (kb + u * blockDim.x < words && col[u] < cols) ? __ldg(inb + e[u].x * cols + col[u]) : e[u].y;
 #pragma unroll
         for (int u = 0; u < kU; ++u)
-          if (on[u]) out[(o + qb + u * stride + lane_q) * out_cols + lane_c] = val[u];
+          if (kb + u * blockDim.x < words) sb[lead + kb + u * blockDim.x] = val[u];
       }
-      continue;
-    }
-    // wider rows: a warp per output row, lanes over its words; kU rows of
-    // a warp in flight at once
-    for (uint32_t qb = wid; qb < c; qb += kU * nwarps) {
-      uint2 e[kU];
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        const uint32_t q = qb + u * nwarps;
-        e[u] = (q < c && o + q < out_cap) ? __ldg(kt + q) : make_uint2(0xffffffffu, 0u);
+      __syncthreads();
+      // aligned middle [k0, k1) by one bulk copy, the ends by plain stores
+      const uint32_t k0 = min((4u - lead) & 3u, words);
+      const uint32_t k1 = k0 + ((words - k0) & ~3u);
+      bool bulk = false;
+      if (k1 > k0) {
+        const uintptr_t ga = (uintptr_t)(dst + k0), sa = (uintptr_t)(sb + lead + k0);
+        bulk = ((ga | sa) & 15u) == 0 && (((k1 - k0) * 4u) & 15u) == 0;
       }
-      for (uint32_t w0 = 0; w0 < out_cols; w0 += 32) {
-        const uint32_t col = w0 + lane;
-        uint32_t val[kU];
-#pragma unroll
-        for (int u = 0; u < kU; ++u)
-          val[u] = (e[u].x != 0xffffffffu && col < cols) ? __ldg(in + (row_begin + e[u].x) * cols + col) : e[u].y;
-#pragma unroll
-        for (int u = 0; u < kU; ++u)
-          if (e[u].x != 0xffffffffu && col < out_cols) out[(o + qb + u * nwarps) * out_cols + col] = val[u];
-      }
+      if (bulk && threadIdx.x == 0) bulk_store(dst + k0, sb + lead + k0, (k1 - k0) * 4u);
+      for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
+        if (!bulk || k < k0 || k >= k1) dst[k] = sb[lead + k];
     }
   }
+  if (threadIdx.x == 0) bulk_wait_all();  // the span is in global memory before the block ends
 }
 
 // Blocks of k_extend_check<ITEMS> one SM holds at once (registers and shared

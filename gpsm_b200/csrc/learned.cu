@@ -198,7 +198,8 @@ __global__ void k_mlp_to_bf16(const float* __restrict__ w, __nv_bfloat16* __rest
 // ---------------------------------------------------------------------------
 // planner: one warp per start vertex runs the greedy order.
 // ---------------------------------------------------------------------------
-constexpr int kPlanWarps = 9;  // up to 8 greedy starts + the scored plain order
+constexpr int kPlanWarps = 9;  // up to 8 greedy starts + the scored plain order (one block each)
+constexpr int kPlanTeam = 8;   // warps of a plan's block: frontier candidates scored 8 at a time
 struct PlanOut {
   int32_t order[kMaxPlanQ];
   float work;     // predicted sum of 2^{L_k} over the intermediate tables (widths 1 .. n-1)
@@ -218,18 +219,22 @@ struct PlanSmem {
   float b2[kHidden];
   float w3[kHidden];
   float b3;
-  float x[kPlanWarps][kFeat];    // features of the candidate a warp scores
-  float h1[kPlanWarps][kHidden];
-  float h2[kPlanWarps][kHidden];
+  float x[kPlanTeam][kFeat];    // features of the candidate a warp scores
+  float h1[kPlanTeam][kHidden];
+  float h2[kPlanTeam][kHidden];
+  float best[kPlanTeam];        // each warp's best candidate of the step
+  uint32_t bv[kPlanTeam];
 };
 
-// One warp per start vertex builds a greedy order; when `fixed` is given,
-// warp `nstarts` scores that order instead (same predictions, no choice).
-// A warp scores the frontier candidates one after another, its lanes
+// One block per start vertex builds a greedy order; when `fixed` is given,
+// block `nstarts` scores that order instead (same predictions, no choice).
+// Each step, the block's warps score the frontier candidates, eight at a
+// time (the i-th candidate in vertex order goes to warp i mod 8), lanes
 // splitting the hidden units; each unit's sum runs over its inputs in the
 // same order as mlp_eval, and lane 0 forms the output sum in order, so the
-// predictions equal mlp_eval's.
-__global__ void __launch_bounds__(32 * kPlanWarps) k_plan(const PlanQuery* __restrict__ Qp,
+// predictions equal mlp_eval's. The step takes the smallest prediction,
+// ties to the smallest vertex, as a scan in vertex order would.
+__global__ void __launch_bounds__(32 * kPlanTeam, 1) k_plan(const PlanQuery* __restrict__ Qp,
                                                           const PlanEdges* __restrict__ E,
                                                           const uint32_t* __restrict__ starts, uint32_t nstarts,
                                                           const int32_t* __restrict__ fixed,
@@ -251,18 +256,18 @@ __global__ void __launch_bounds__(32 * kPlanWarps) k_plan(const PlanQuery* __res
   }
   if (threadIdx.x == 0) S.b3 = wf[kB3];
   __syncthreads();
-  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const bool follow = fixed && wid == nstarts;
-  if (wid >= nstarts && !follow) return;
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, plan = blockIdx.x;
+  const bool follow = fixed && plan == nstarts;
+  if (plan >= nstarts && !follow) return;  // block-uniform
   const PlanQuery& Q = *Qp;
   const uint32_t n = Q.n;
-  PlanOut& O = outs[wid];
+  PlanOut& O = outs[plan];
   uint64_t P[2] = {0, 0};
-  const uint32_t v0 = follow ? (uint32_t)fixed[0] : starts[wid];
+  const uint32_t v0 = follow ? (uint32_t)fixed[0] : starts[plan];
   P[v0 >> 6] |= 1ULL << (v0 & 63);
-  if (lane == 0) O.order[0] = (int32_t)v0;
+  if (threadIdx.x == 0) O.order[0] = (int32_t)v0;
   float L = Q.log_cand[v0];
-  if (lane == 0) O.logsize[0] = L;
+  if (threadIdx.x == 0) O.logsize[0] = L;
   float work = exp2f(L), peak = exp2f(L) * 4.f;
   float* x = S.x[wid];
   float* h1 = S.h1[wid];
@@ -270,10 +275,12 @@ __global__ void __launch_bounds__(32 * kPlanWarps) k_plan(const PlanQuery* __res
   for (uint32_t k = 1; k < n; ++k) {
     float best = 1e30f;
     uint32_t bv = 0xffffffffu;
-    for (uint32_t v = 0; v < n; ++v) {  // warp-uniform
+    uint32_t seen = 0;                   // frontier candidates so far (block-uniform)
+    for (uint32_t v = 0; v < n; ++v) {  // block-uniform
       if (pq_has(P, v)) continue;
       if (!((Q.adj[v][0] & P[0]) | (Q.adj[v][1] & P[1]))) continue;
       if (follow && v != (uint32_t)fixed[k]) continue;
+      if ((seen++ % kPlanTeam) != wid) continue;  // another warp scores it (warp-uniform)
       if (lane == 0) step_features(Q, *E, P, k, v, x);
       __syncwarp();
       float a0 = S.b1[lane], a1 = S.b1[lane + 32];
@@ -309,19 +316,33 @@ __global__ void __launch_bounds__(32 * kPlanWarps) k_plan(const PlanQuery* __res
         bv = v;
       }
     }
+    // the block's best: the smallest prediction, ties to the smallest vertex
+    if (lane == 0) {
+      S.best[wid] = best;
+      S.bv[wid] = bv;
+    }
+    __syncthreads();
+    best = 1e30f;
+    bv = 0xffffffffu;
+    for (int w = 0; w < kPlanTeam; ++w)
+      if (S.bv[w] != 0xffffffffu && (S.best[w] < best || (S.best[w] == best && S.bv[w] < bv))) {
+        best = S.best[w];
+        bv = S.bv[w];
+      }
+    __syncthreads();  // S.best / S.bv are rewritten next step
     if (bv == 0xffffffffu) break;  // disconnected (rejected earlier)
     P[bv >> 6] |= 1ULL << (bv & 63);
-    if (lane == 0) O.order[k] = (int32_t)bv;
+    if (threadIdx.x == 0) O.order[k] = (int32_t)bv;
     L += best;
     L = L < 0.f ? 0.f : L;
-    if (lane == 0) O.logsize[k] = L;
+    if (threadIdx.x == 0) O.logsize[k] = L;
     const float rows = exp2f(L);
     // the final table holds the embeddings, the same in every order (and,
     // under a cap, the same number of rows): it does not rank orders
     if (k + 1 < n) work += rows;
     peak = fmaxf(peak, rows * 4.f * (float)(k + 1));
   }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     O.work = work;
     O.peak = peak;
   }
@@ -494,8 +515,8 @@ void model_predict(Model* M, const float* x, uint32_t n, float* y) {
 void launch_plan(cudaStream_t s, const Model* M, const PlanQuery* d_q, const PlanEdges* d_e, const uint32_t* d_starts,
                  uint32_t nstarts, const int32_t* d_fixed, void* d_out) {
   nstarts = std::min<uint32_t>(nstarts, kPlanWarps - 1);
-  const uint32_t warps = std::max<uint32_t>(1, nstarts + (d_fixed ? 1 : 0));
-  k_plan<<<1, 32 * warps, 0, s>>>(d_q, d_e, d_starts, nstarts, d_fixed, M->wb, M->w, (PlanOut*)d_out);
+  const uint32_t plans = std::max<uint32_t>(1, nstarts + (d_fixed ? 1 : 0));
+  k_plan<<<plans, 32 * kPlanTeam, 0, s>>>(d_q, d_e, d_starts, nstarts, d_fixed, M->wb, M->w, (PlanOut*)d_out);
   GPSM_LAUNCHED();
 }
 

@@ -307,7 +307,7 @@ typedef struct gpsm_tuning {
   uint64_t race_share;         /* learned order: first work share (candidates) when the learned plan
                                   and the plain order take turns (default 2^28) */
   uint32_t ext_items;          /* candidates per thread of the join check kernel: 4 or 8 (default 4) */
-  uint32_t pad;
+  uint32_t filter_team;        /* lanes per candidate in the refinement steps: 8 or 32 (default 8) */
 } gpsm_tuning;
 int gpsm_set_tuning(const gpsm_tuning* t);
 int gpsm_get_tuning(gpsm_tuning* t);

@@ -348,24 +348,43 @@ def run_ours(args):
     e2e_qs = [q for s in e2e_slices for q in wl.queries[bounds[s][0]:bounds[s][1]]]
     h2d = sum(int(q.labels.nbytes + q.edges.nbytes) for q in e2e_qs)
     barrier(pg)
-    srv = G.Server(dg, slots=slots, cap=cap, order=args.order if args.order == "learned" else None,
-                   model=model, collect_rows=True, work_cap=work_cap)
-    for q in e2e_qs:  # untimed: grows the pool of page-locked result blocks
-        srv.submit(q)
-    for _ in e2e_qs:
-        srv.wait_any()
+    # the batch slots and the one-slot plain leg keep their arenas: the
+    # server's slots share most of what is left. A failure here is reported
+    # in the line (every rank still takes the same collective steps).
+    import torch
+    free_b, _ = torch.cuda.mem_get_info(local)
+    e2e_err, srv = None, None
+    d2h, e2e_rows = 0, 0
+    try:
+        srv = G.Server(dg, slots=slots, cap=cap, order=args.order if args.order == "learned" else None,
+                       model=model, collect_rows=True, work_cap=work_cap,
+                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)))
+        for q in e2e_qs:  # untimed: grows the pool of page-locked result blocks
+            srv.submit(q)
+        for _ in e2e_qs:
+            srv.wait_any()
+    except G.GpsmError as ex:
+        e2e_err = str(ex)
     barrier(pg)
     t1 = time.perf_counter()
-    d2h, e2e_rows = 0, 0
-    for q in e2e_qs:
-        srv.submit(q)
-    for _ in e2e_qs:  # results as they finish, so host memory holds only what is still running
-        _, r = srv.wait_any()
-        d2h += r["table"].nbytes
-        e2e_rows += int(r["rows"])
-        del r
+    if e2e_err is None:
+        try:
+            for q in e2e_qs:
+                srv.submit(q)
+            for _ in e2e_qs:  # results as they finish, so host memory holds only what is still running
+                _, r = srv.wait_any()
+                d2h += r["table"].nbytes
+                e2e_rows += int(r["rows"])
+                del r
+        except G.GpsmError as ex:
+            e2e_err = str(ex)
     e2e_wall = max_over_ranks(pg, time.perf_counter() - t1)
-    srv.close()
+    if srv is not None:
+        try:
+            srv.close()
+        except G.GpsmError:
+            pass
+    e2e_failed = max_over_ranks(pg, 1.0 if e2e_err else 0.0) > 0
     e2e_q = sum_over_ranks(pg, len(e2e_qs))
     e2e_d2h = sum_over_ranks(pg, d2h)
 
@@ -424,6 +443,10 @@ def run_ours(args):
             "aborted_at_work_cap": aborted,
             "p50_ms": float(np.percentile(qms_all, 50)) if qms_all else None,
             "p99_ms": float(np.percentile(qms_all, 99)) if qms_all else None,
+            "step_ms": [round(x, 1) for x in step_ms],
+            # summed per-query device time over slots x step time: how full the
+            # slots were (a slice whose last query runs alone lowers it)
+            "slot_fill": float(sum(qms_all) / (slots * sum(step_ms))) if step_ms else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "kernel": "join step (k_locate + k_extend_check + k_scan_u32 + k_extend_write)",
@@ -435,11 +458,13 @@ def run_ours(args):
                          "join_steps": tot["join_steps"]},
             "cpu_baseline": cpu,
             "reference_build": refb,
-            "e2e": {"value": e2e_q / e2e_wall, "unit": "queries/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": int(e2e_d2h / max(world, 1)), "rows_per_s": e2e_rows / e2e_wall,
-                    "d2h_gb_per_s": e2e_d2h / 1e9 / e2e_wall,
-                    "basis": "request server, slice 0 (host query arrays in, every embedding row to host "
-                             "memory, results taken as they finish), after one untimed pass"},
+            "e2e": ({"value": None, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 0,
+                     "error": e2e_err or "failed on another rank"} if e2e_failed else
+                    {"value": e2e_q / e2e_wall, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                     "d2h_bytes_per_step": int(e2e_d2h / max(world, 1)), "rows_per_s": e2e_rows / e2e_wall,
+                     "d2h_gb_per_s": e2e_d2h / 1e9 / e2e_wall,
+                     "basis": "request server, slice 0 (host query arrays in, every embedding row to host "
+                              "memory, results taken as they finish), after one untimed pass"}),
             "gpu_launches": int(sum_over_ranks(pg, tot["launches"])),
             "clocks": clk,
             "wall_s": wall,

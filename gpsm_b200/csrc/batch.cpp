@@ -199,9 +199,14 @@ struct Server {
   const DeviceGraph* g = nullptr;
   std::vector<Workspace*> ws;
   std::vector<std::thread> threads;
+  std::thread completer;  // publishes requests whose rows are still being copied
   std::mutex mu;
-  std::condition_variable cv_q, cv_done, cv_mem;
+  std::condition_variable cv_q, cv_done, cv_mem, cv_drain;
   std::deque<Request*> queue;
+  // requests whose joins are done and whose last row copies are still
+  // running, with the event recorded after those copies (completion order)
+  std::deque<std::pair<Request*, cudaEvent_t>> draining;
+  bool slots_done = false;
   std::map<uint64_t, Request*> all;
   std::deque<uint64_t> finished;  // tickets in completion order (for wait_any)
   uint64_t next_id = 1;
@@ -268,6 +273,7 @@ struct Server {
           mo.release = &Server::release_cb;
           mo.admit_ctx = &ctx;
           mo.collect_rows = collect;
+          mo.defer_copies = collect;
           rc = run_query(*ws[s], *g, Q, mo, R);
         } else {
           set_last_error(err);
@@ -275,9 +281,14 @@ struct Server {
       } catch (const CudaError& e) {
         rc = e.err == cudaErrorMemoryAllocation ? GPSM_ERR_NOMEM : GPSM_ERR_CUDA;
       }
+      if (R.copies_done && rc != GPSM_OK) {  // no request takes the rows: let the copies end here
+        cudaEventSynchronize(R.copies_done);
+        cudaEventDestroy(R.copies_done);
+        R.copies_done = nullptr;
+      }
+      bool drain = false;
       {
         std::lock_guard<std::mutex> lk(mu);
-        r->status = rc;
         if (rc != GPSM_OK) r->err = last_error();
         r->rows = R.rows;
         r->capped = R.capped ? 1 : (R.stats.aborted ? 2 : 0);
@@ -286,8 +297,48 @@ struct Server {
           r->result = std::move(R.host_rows);
           r->id2pos = R.id2pos;
         }
-        r->t_end = now_ms();
         --active;
+        if (R.copies_done) {
+          // the slot takes its next request while the rows finish copying
+          // (the next query's joins wait for them on the device)
+          draining.emplace_back(r, R.copies_done);
+          drain = true;
+        } else {
+          r->status = rc;
+          r->t_end = now_ms();
+          finished.push_back(r->id);
+        }
+      }
+      if (drain) cv_drain.notify_one();
+      else cv_done.notify_all();
+    }
+  }
+
+  // Waits for each draining request's copies in turn and publishes it.
+  void complete_loop(int device) {
+    cudaSetDevice(device);
+    for (;;) {
+      std::pair<Request*, cudaEvent_t> d;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_drain.wait(lk, [&] { return slots_done || !draining.empty(); });
+        if (draining.empty()) return;  // the slots have stopped and nothing is left
+        d = draining.front();
+      }
+      const cudaError_t e = cudaEventSynchronize(d.second);
+      cudaEventDestroy(d.second);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        draining.pop_front();
+        Request* r = d.first;
+        if (e != cudaSuccess) {
+          r->status = GPSM_ERR_CUDA;
+          r->err = std::string("copy of result rows: ") + cudaGetErrorString(e);
+          r->result = HostRows();
+        } else {
+          r->status = GPSM_OK;
+        }
+        r->t_end = now_ms();
         finished.push_back(r->id);
       }
       cv_done.notify_all();
@@ -362,6 +413,7 @@ int gpsm_server_create(gpsm_graph_t g, uint32_t slots, uint64_t memory_budget, u
     for (uint32_t i = 0; i < slots; ++i) S->ws.push_back(workspace_create(g->g->device, arena, 1u << 20));
     S->budget = memory_budget ? memory_budget : arena * slots;
     for (uint32_t i = 0; i < slots; ++i) S->threads.emplace_back(&Server::slot_loop, S, i);
+    S->completer = std::thread(&Server::complete_loop, S, g->g->device);
     gpsm_server_s* h = new gpsm_server_s();
     h->s = S;
     *out = h;
@@ -485,6 +537,12 @@ int gpsm_server_destroy(gpsm_server_t h) {
   S->cv_q.notify_all();
   S->cv_mem.notify_all();
   for (auto& t : S->threads) t.join();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->slots_done = true;
+  }
+  S->cv_drain.notify_all();
+  S->completer.join();  // every draining request is published first
   for (Workspace* w : S->ws) workspace_free(w);
   for (auto& kv : S->all) delete kv.second;
   delete S;

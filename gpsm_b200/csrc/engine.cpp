@@ -671,10 +671,19 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   uint32_t* nbrs = C.F.nbrs;
   const uint64_t nbrs_total = C.F.nbrs_total;
   auto bm_of = [&](uint32_t u) { return C.F.bm + (size_t)u * W; };
-  // whatever path leaves this attempt, its row copies to the host have ended
+  // an earlier attempt's copies into the host block end before it is reused
+  if (R.copies_pending) {
+    GPSM_CUDA(cudaStreamSynchronize(ws.copy_stream));
+    R.copies_pending = false;
+  }
+  // whatever path leaves this attempt, its row copies to the host have
+  // ended, unless it returns normally with copies deferred to the caller
   struct CopiesDone {
     Workspace& w;
-    ~CopiesDone() { cudaStreamSynchronize(w.copy_stream); }
+    bool armed = true;
+    ~CopiesDone() {
+      if (armed) cudaStreamSynchronize(w.copy_stream);
+    }
   } copies_done{ws};
   hit_limit = false;
   ws.arena.used = join_mark;
@@ -743,7 +752,9 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   uint32_t max_nb = 1;
   for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
   // per-row scratch: 16 B driver + 8 B offset + 16 B per placed neighbour
-  js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, (1ull << 30) / (16ull * max_nb)), 4096);
+  // (at most 1 GiB and a sixteenth of the arena)
+  const uint64_t row_scratch = std::min<uint64_t>(1ull << 30, ws.arena.size / 16);
+  js.rows = std::max<uint64_t>(std::min<uint64_t>(opt.step_rows, row_scratch / (16ull * max_nb)), 4096);
   js.rng_entries = js.rows * max_nb;
   js.drv = arena_alloc<uint4>(ws, js.rows);
   js.rng = arena_alloc<uint4>(ws, js.rng_entries);
@@ -793,13 +804,26 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   if (qn > 2) L[2].buf = stack;
   uint64_t res_cap = std::max<uint64_t>(std::min<uint64_t>(opt.result_rows, cap), 1);
   if (qn > 1) res_cap = std::max<uint64_t>(res_cap, std::min<uint64_t>(cap, min_rows));
-  uint32_t* res_buf = arena_alloc<uint32_t>(ws, res_cap * qn);
-  // rows bound for a page-locked block get a second result buffer: the
-  // joins fill one while the other is copied out on the copy stream
-  uint32_t* res_bufs[2] = {res_buf, nullptr};
+  // rows bound for a page-locked block get two result buffers: the joins
+  // fill one while the other is copied out on the copy stream. With
+  // deferred copies they are the workspace's persistent pair, whose copies
+  // from the previous query may still run: the stream waits for them.
+  const bool async_rows = opt.collect_rows && !opt.keep_on_device && R.host_rows.pinned();
+  const bool ring = async_rows && opt.defer_copies && ws.res_ring_words &&
+                    std::min<uint64_t>(res_cap, ws.res_ring_words / qn) >= std::min<uint64_t>(cap, min_rows);
+  uint32_t* res_bufs[2] = {nullptr, nullptr};
+  if (ring) {
+    res_cap = std::min<uint64_t>(res_cap, ws.res_ring_words / qn);
+    res_bufs[0] = ws.res_ring[0];
+    res_bufs[1] = ws.res_ring[1];
+    GPSM_CUDA(cudaStreamWaitEvent(s, ws.ev_copied[0], 0));
+    GPSM_CUDA(cudaStreamWaitEvent(s, ws.ev_copied[1], 0));
+  } else {
+    res_bufs[0] = arena_alloc<uint32_t>(ws, res_cap * qn);
+    if (async_rows) res_bufs[1] = (uint32_t*)ws.arena.alloc(std::max<uint64_t>(res_cap * qn, 1) * sizeof(uint32_t));
+  }
+  uint32_t* res_buf = res_bufs[0];
   int res_cur = 0;
-  if (opt.collect_rows && !opt.keep_on_device && R.host_rows.pinned())
-    res_bufs[1] = (uint32_t*)ws.arena.alloc(std::max<uint64_t>(res_cap * qn, 1) * sizeof(uint32_t));
   // directed mode: final rows land in a staging buffer and only those whose
   // query edges are directed, labelled data edges move to the result
   uint32_t* stage = nullptr;
@@ -1024,6 +1048,10 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     R.d_rows = res_buf;
     R.d_rows_count = res_used;
   }
+  if (ring) {  // the caller waits for the copies (run_query hands them on)
+    copies_done.armed = false;
+    R.copies_pending = true;
+  }
   return GPSM_OK;
 }
 
@@ -1042,6 +1070,17 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   }
   ws.dirty = true;
   ws.arena.reset();
+  if (opt.defer_copies && opt.collect_rows && !opt.keep_on_device) ws.result_ring();
+  // copies still running into R.host_rows end before any path but the
+  // successful one leaves (that one hands them to the caller as an event)
+  struct PendingCopies {
+    Workspace& w;
+    MatchResult& r;
+    ~PendingCopies() {
+      if (r.copies_pending) cudaStreamSynchronize(w.copy_stream);
+      r.copies_pending = false;
+    }
+  } pending_copies{ws, R};
   R.cols = qn;
   GPSM_CUDA(cudaEventRecord(ws.ev0, s));
   GPSM_CUDA(cudaMemsetAsync(ws.d_flags, 0, 64 * sizeof(uint32_t), s));
@@ -1173,6 +1212,11 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   R.stats.device_ms = ms;
   R.stats.filter_ms = ms_f;
   R.stats.join_ms = ms - ms_f;
+  if (R.copies_pending) {
+    GPSM_CUDA(cudaEventCreateWithFlags(&R.copies_done, cudaEventDisableTiming | cudaEventBlockingSync));
+    GPSM_CUDA(cudaEventRecord(R.copies_done, ws.copy_stream));
+    R.copies_pending = false;
+  }
   return GPSM_OK;
 }
 

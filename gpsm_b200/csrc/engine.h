@@ -75,6 +75,13 @@ struct MatchOptions {
   std::vector<uint32_t> edge_labels;    // per query edge in file order (empty = all 1)
   uint64_t memory_budget = 0;           // bytes; predicted peak above it -> plain order (0 = arena size)
   uint64_t work_cap = 0;                // candidates the joins may scan before stopping, all attempts (0 = none)
+  // Rows bound for a page-locked block leave through the workspace's two
+  // persistent result buffers, and run_query returns while the last copies
+  // are still running: R.copies_done is then an event the caller waits on
+  // (and destroys) before reading R.host_rows. The next query on the same
+  // workspace waits for those copies on the device before writing the
+  // buffers, so the slot's next filter overlaps them.
+  bool defer_copies = false;
   // Admission hook (serving): called after the order is chosen, before the
   // joins, with the bytes the joins are predicted to use; returns false to
   // refuse (GPSM_ERR_BUDGET). release() gets the same bytes back afterwards.
@@ -164,6 +171,8 @@ struct MatchResult {
   uint32_t* d_rows = nullptr;       // rows still on the device (arena memory; valid until the next query)
   uint64_t d_rows_count = 0;        // rows in d_rows (after host_rows)
   MatchStats stats;
+  bool copies_pending = false;      // copies into host_rows may still run on the copy stream
+  cudaEvent_t copies_done = nullptr;  // defer_copies: recorded after the last copy (the caller destroys it)
 };
 
 int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const MatchOptions& opt, MatchResult& R);

@@ -304,7 +304,11 @@ struct Team {
 // Explore one candidate mu of u with team T: every neighbour mv with the
 // target's label and degree >= the target's enters C(v); mu leaves C(u) at
 // the first target that gets none (match/Match.cu:594-598) and later
-// targets are skipped.
+// targets are skipped. Each lane takes kScanU neighbours a round: their
+// list entries, then their (label, degree), then their bitmap words are
+// loaded together, so a long run costs a quarter of the dependent rounds.
+constexpr uint32_t kScanU = 4;
+
 template <int G>
 __device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
                                             const uint32_t* s_tgt, uint32_t ntgt, uint32_t* __restrict__ bm,
@@ -316,14 +320,31 @@ __device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uin
     bool any = false;
     uint32_t rb, re;
     const uint32_t* cl = scan_range_team<G>(g, mu, lv, b, e, &rb, &re);
-    for (uint32_t j = rb + T.rank; j < re; j += T.size) {
-      const uint32_t mv = cl[j];
-      const uint2 ld = g.labdeg[mv];
-      if (ld.x == lv && ld.y >= dv) {
+    for (uint32_t j0 = rb + T.rank; j0 < re; j0 += kScanU * T.size) {
+      uint32_t mv[kScanU];
+      bool in[kScanU];
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        const uint32_t j = j0 + k * T.size;
+        in[k] = j < re;
+        mv[k] = in[k] ? cl[j] : 0u;
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        if (!in[k]) continue;
+        const uint2 ld = g.labdeg[mv[k]];
+        in[k] = ld.x == lv && ld.y >= dv;
+      }
+      uint32_t have[kScanU];
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) have[k] = in[k] ? bmv[mv[k] >> 5] : 0u;
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        if (!in[k]) continue;
         // popular vertices are set by many candidates: skip the atomic when
         // the bit is already there (a stale read only costs a spare atomic)
-        const uint32_t bit = 1u << (mv & 31);
-        if (!(bmv[mv >> 5] & bit)) atomicOr(&bmv[mv >> 5], bit);
+        const uint32_t bit = 1u << (mv[k] & 31);
+        if (!(have[k] & bit)) atomicOr(&bmv[mv[k] >> 5], bit);
         any = true;
       }
     }
@@ -335,7 +356,9 @@ __device__ __forceinline__ void explore_one(const GraphView& g, uint32_t mu, uin
 }
 
 // Refine one candidate mu of u with team T: mu stays only if every target
-// x has a candidate among mu's neighbours (match/Match.cu:761-808).
+// x has a candidate among mu's neighbours (match/Match.cu:761-808). The
+// first round looks at one neighbour per lane (most candidates that stay
+// hit there); later rounds at kScanU per lane with their loads together.
 template <int G>
 __device__ __forceinline__ void refine_one(const GraphView& g, uint32_t mu, uint32_t b, uint32_t e,
                                            const uint32_t* s_tgt, uint32_t ntgt, const uint32_t* __restrict__ bm,
@@ -346,13 +369,20 @@ __device__ __forceinline__ void refine_one(const GraphView& g, uint32_t mu, uint
     bool found = false;
     uint32_t rb, re;
     const uint32_t* cl = scan_range_team<G>(g, mu, s_tgt[2 * t + 1], b, e, &rb, &re);
-    for (uint32_t j0 = rb; j0 < re && !found; j0 += T.size) {
-      const uint32_t j = j0 + T.rank;
-      bool hit = false;
-      if (j < re) {
-        const uint32_t mv = cl[j];
-        hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+    uint32_t per = 1;  // neighbours per lane this round
+    for (uint32_t j0 = rb; j0 < re && !found; j0 += per * T.size, per = kScanU) {
+      uint32_t mv[kScanU];
+      bool in[kScanU];
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        const uint32_t j = j0 + k * T.size + T.rank;
+        in[k] = k < per && j < re;
+        mv[k] = in[k] ? cl[j] : 0u;
       }
+      bool hit = false;
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k)
+        if (in[k]) hit |= ((bmv[mv[k] >> 5] >> (mv[k] & 31)) & 1u) != 0;
       found = T.any(hit);
     }
     if (!found) {

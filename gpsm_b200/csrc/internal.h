@@ -163,6 +163,24 @@ struct Workspace {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_res[2] = {nullptr, nullptr};     // buffer k written (on stream)
   cudaEvent_t ev_copied[2] = {nullptr, nullptr};  // buffer k copied out (on copy_stream)
+  // Two result buffers that outlive a query (carved once from the top of
+  // the arena, which shrinks by their size): a query's last copies out of
+  // them may still run while the slot's next query starts; its joins wait
+  // for those copies on the device (ev_copied) before writing the buffers.
+  static constexpr size_t kRingBytes = 512ull << 20;  // per buffer
+  uint32_t* res_ring[2] = {nullptr, nullptr};
+  uint64_t res_ring_words = 0;  // words per buffer (0: not carved)
+  // The pair, carved at the first call; false when the arena is too small
+  // to give it up (the caller then uses per-query buffers).
+  bool result_ring() {
+    if (res_ring_words) return true;
+    if (arena.used != 0 || arena.size < 8 * kRingBytes) return false;
+    arena.size -= 2 * kRingBytes;
+    res_ring[0] = reinterpret_cast<uint32_t*>(arena.base + arena.size);
+    res_ring[1] = reinterpret_cast<uint32_t*>(arena.base + arena.size + kRingBytes);
+    res_ring_words = kRingBytes / sizeof(uint32_t);
+    return true;
+  }
 };
 
 // Copies `words` 32-bit words from device memory to pageable host memory

@@ -389,12 +389,17 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
 
 // Bulk copy shared -> global on the async (TMA) engine, in a bulk group.
 // Both addresses and the size must be multiples of 16 bytes: callers check.
+// Every thread that wrote the source calls proxy_fence_shared() before the
+// barrier that precedes this.
 __device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(ssrc);
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst), "r"(s), "r"(bytes)
                : "memory");
   asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+// Makes this thread's shared-memory writes visible to the async proxy.
+__device__ __forceinline__ void proxy_fence_shared() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 // Waits until at most N bulk groups of this thread still read shared memory.
 template <int N>
@@ -405,21 +410,22 @@ __device__ __forceinline__ void bulk_wait_read() {
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
 constexpr uint32_t kWriteStage = 4096;  // words per staging buffer (two buffers)
+constexpr uint32_t kWriteRows = 1024;   // rows per chunk at most (their kept pairs are staged)
 
 // Block per tile (grid-stride): the tile's kept rows go to output rows
 // tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
 // written and clears the next step's state; each tile's count is cleared
 // once read, so the next step's check pass starts from zero counts.
 // The tile's output is one contiguous span. It is built in chunks of whole
-// rows in shared memory, one output word per thread at a time (its row by a
-// multiply-high with the precomputed reciprocal of the row width, exact for
-// these ranges; kU words' loads in flight per thread: the kept pair, then
-// the input row's word) and each chunk leaves by one bulk copy on the async
-// engine; the chunk is laid out so that every word has the
-// same 16-byte phase in shared memory as in the output, so the aligned middle
-// goes in one copy and at most three words at each end by plain stores. Two
-// staging buffers alternate: gathering the next chunk overlaps the copy of
-// the previous one.
+// rows in shared memory: the chunk's kept (row, value) pairs are staged
+// first (one coalesced load per row), then each thread fills one output
+// word at a time (its row by a multiply-high with the precomputed reciprocal
+// of the row width, exact for these ranges; kU input words' loads in flight
+// per thread), and the chunk leaves by one bulk copy on the async engine.
+// The chunk is laid out so that every word has the same 16-byte phase in
+// shared memory as in the output, so the aligned middle goes in one copy
+// and at most three words at each end by plain stores. Two staging buffers
+// alternate: gathering the next chunk overlaps the copy of the previous one.
 __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
                                                          unsigned long long row_begin, const uint2* __restrict__ kept,
                                                          uint32_t* __restrict__ tile_cnt,
@@ -429,8 +435,10 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
                                                          StepState* __restrict__ next) {
   constexpr int kU = 4;
   __shared__ __align__(128) uint32_t sbuf[2][kWriteStage + 4];
+  __shared__ uint2 s_kept[kWriteRows];
   const uint32_t out_cols = cols + 1;
-  const uint32_t chunk_rows = kWriteStage / out_cols;  // >= 31: rows hold at most 128 words
+  // >= 31 rows (rows hold at most 128 words), <= kWriteRows
+  const uint32_t chunk_rows = min(kWriteStage / out_cols, kWriteRows);
   // ceil(2^32 / out_cols): __umulhi(k, recip) == k / out_cols for every
   // k < 2^32 / out_cols (here k < kWriteStage)
   const uint32_t recip = (uint32_t)((0x100000000ull + out_cols - 1) / out_cols);
@@ -455,6 +463,8 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
       const uint32_t lead = (uint32_t)(((uintptr_t)dst >> 2) & 3);  // dst's word phase within 16 bytes
       uint32_t* sb = sbuf[chunk_no & 1];
       if (threadIdx.x == 0) bulk_wait_read<1>();  // the copy that last read this buffer is done with it
+      __syncthreads();  // ... and the previous chunk's gather no longer reads s_kept
+      for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) s_kept[i] = __ldg(kt + q0 + i);
       __syncthreads();
       for (uint32_t kb = threadIdx.x; kb < words; kb += kU * blockDim.x) {
         uint32_t col[kU], val[kU];
@@ -464,15 +474,17 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
           const uint32_t k = kb + u * blockDim.x;
           const uint32_t q = __umulhi(k, recip);
           col[u] = k - q * out_cols;
-          e[u] = k < words ? __ldg(kt + q0 + q) : make_uint2(0u, 0u);
+          e[u] = k < words ? s_kept[q] : make_uint2(0u, 0u);
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u)
-          val[u] = (kb + u * blockDim.x < words && col[u] < cols) ? __ldg(inb + e[u].x * cols + col[u]) : e[u].y;
+          val[u] = (kb + u * blockDim.x < words && col[u] < cols) ? __ldg(inb + (size_t)e[u].x * cols + col[u])
+                                                                  : e[u].y;
 #pragma unroll
         for (int u = 0; u < kU; ++u)
           if (kb + u * blockDim.x < words) sb[lead + kb + u * blockDim.x] = val[u];
       }
+      proxy_fence_shared();
       __syncthreads();
       // aligned middle [k0, k1) by one bulk copy, the ends by plain stores
       const uint32_t k0 = min((4u - lead) & 3u, words);
@@ -482,9 +494,15 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
         const uintptr_t ga = (uintptr_t)(dst + k0), sa = (uintptr_t)(sb + lead + k0);
         bulk = ((ga | sa) & 15u) == 0 && (((k1 - k0) * 4u) & 15u) == 0;
       }
-      if (bulk && threadIdx.x == 0) bulk_store(dst + k0, sb + lead + k0, (k1 - k0) * 4u);
-      for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
-        if (!bulk || k < k0 || k >= k1) dst[k] = sb[lead + k];
+      if (bulk) {
+        if (threadIdx.x == 0) bulk_store(dst + k0, sb + lead + k0, (k1 - k0) * 4u);
+        // head: threads 0..k0-1; tail (words - k1 <= 3 words): threads 4..
+        const uint32_t t = threadIdx.x;
+        if (t < k0) dst[t] = sb[lead + t];
+        else if (t >= 4 && t - 4 < words - k1) dst[k1 + t - 4] = sb[lead + k1 + t - 4];
+      } else {
+        for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) dst[k] = sb[lead + k];
+      }
     }
   }
   if (threadIdx.x == 0) bulk_wait_all();  // the span is in global memory before the block ends

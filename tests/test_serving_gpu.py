@@ -100,3 +100,19 @@ def test_wait_any_returns_every_request_once_in_completion_order(gpu, mixed):
     with pytest.raises(gpu.GpsmError):
         srv.wait_any(timeout=0.0)
     srv.close()
+
+
+def test_rows_copied_while_the_slot_moves_on(gpu, mixed):
+    """Small device result buffers (2,000 rows): every capped query flushes
+    its rows in many copies through the slot's two persistent buffers, and
+    a slot starts its next query while the last copies of the previous one
+    still run. Every request's rows equal a sequential match."""
+    g, qs, dg = mixed
+    srv = gpu.Server(dg, slots=2, cap=50000, collect_rows=True, result_rows=2000)
+    tickets = {srv.submit(q)[0]: q for q in qs + qs[:6]}
+    for _ in range(len(tickets)):
+        (tid, _), r = srv.wait_any()
+        ref = gpu.match(dg, tickets[tid], cap=50000)
+        assert r["status"] == 0 and r["rows"] == ref.count
+        assert np.array_equal(r["table"][:, r["id_map"]], ref.embeddings())
+    srv.close()

@@ -358,7 +358,7 @@ def run_ours(args):
     try:
         srv = G.Server(dg, slots=slots, cap=cap, order=args.order if args.order == "learned" else None,
                        model=model, collect_rows=True, work_cap=work_cap,
-                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)))
+                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)) >> 21 << 21)
         for q in e2e_qs:  # untimed: grows the pool of page-locked result blocks
             srv.submit(q)
         for _ in e2e_qs:

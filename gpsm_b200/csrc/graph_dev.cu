@@ -298,6 +298,7 @@ void graph_free(DeviceGraph* g) {
 
 Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) {
   GPSM_CUDA(cudaSetDevice(device));
+  arena_bytes = std::max<size_t>(arena_bytes & ~((size_t(2) << 20) - 1), size_t(2) << 20);  // whole 2 MiB units
   Workspace* ws = new Workspace();
   ws->device = device;
   try {

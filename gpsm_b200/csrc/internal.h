@@ -175,7 +175,8 @@ struct Workspace {
   bool result_ring() {
     if (res_ring_words) return true;
     if (arena.used != 0 || arena.size < 8 * kRingBytes) return false;
-    arena.size -= 2 * kRingBytes;
+    // the pair starts on a 4 KiB boundary whatever the arena's size
+    arena.size = (arena.size - 2 * kRingBytes) & ~(size_t)4095;
     res_ring[0] = reinterpret_cast<uint32_t*>(arena.base + arena.size);
     res_ring[1] = reinterpret_cast<uint32_t*>(arena.base + arena.size + kRingBytes);
     res_ring_words = kRingBytes / sizeof(uint32_t);

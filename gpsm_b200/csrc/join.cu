@@ -575,6 +575,11 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
     set_last_error("join step: more rows than the step scratch holds");
     throw CudaError{cudaErrorInvalidValue, "join rows"};
   }
+  // word arrays on 4-byte and pair arrays on 8-byte boundaries, or no launch
+  if ((((uintptr_t)in | (uintptr_t)out) & 3u) || ((uintptr_t)js.kept & 7u)) {
+    set_last_error("join step: misaligned row buffer");
+    throw CudaError{cudaErrorInvalidValue, "join alignment"};
+  }
   const uint64_t ltiles = (nrows + kLocBlock - 1) / kLocBlock;
   Lookback lb1 = next_lb(ws, ltiles);
   k_locate<<<(uint32_t)ltiles, kLocBlock, 0, ws.stream>>>(in, in_cols, row_begin, nrows, d_back, nb, nbrs_total,

@@ -108,7 +108,9 @@ def test_rows_copied_while_the_slot_moves_on(gpu, mixed):
     a slot starts its next query while the last copies of the previous one
     still run. Every request's rows equal a sequential match."""
     g, qs, dg = mixed
-    srv = gpu.Server(dg, slots=2, cap=50000, collect_rows=True, result_rows=2000)
+    # an arena size that is no multiple of anything: the persistent result
+    # buffers carved from its top must still start on an aligned address
+    srv = gpu.Server(dg, slots=2, cap=50000, collect_rows=True, result_rows=2000, slot_arena=(4 << 30) + 12345)
     tickets = {srv.submit(q)[0]: q for q in qs + qs[:6]}
     for _ in range(len(tickets)):
         (tid, _), r = srv.wait_any()

@@ -1,10 +1,11 @@
 """Autotuner for the engine's launch choices.
 
-    python -m gpsm_b200.autotune [--workload rmat22] [--queries 24] [--out gpsm_b200/data/tuning.json]
+    python -m gpsm_b200.autotune [--workload rmat22] [--slices 0,7] [--out gpsm_b200/data/tuning.json]
 
-Times a sample of the workload's queries in the learned join order (device
-time of the whole batch, best of two runs after a warm-up) under every
-combination of:
+Times whole slices of the benchmark batch (1/20 of the 4,096 queries each,
+the bench's own steps, with its cap and work cap) in the learned join order
+on the tuned number of slots (device time of the batch, best of two runs
+after a warm-up) under every combination of:
   heavy_degree       candidates above it get a block each (filter kernels)
   ext_blocks_per_sm  persistent join-check blocks per SM (at most what the
                      SM holds for the kernel's register count)
@@ -15,12 +16,13 @@ combination of:
   step_cands         candidates one join step may admit
   slots              engine slots running queries at once
 and writes the fastest combination to --out; gpsm_b200.init() applies it.
+Whole slices keep the queries that run to the work cap: they decide the
+step budget (a budget whose scratch outgrows L2 slows every long query) and
+a sample of quick queries alone picked the wrong one. --queries N instead
+times N quick queries (device time under --max-ms each).
 Slot counts are compared one process each (--slots; a process sizes every
 slot pool from the memory left free when the pool is created, so a second
 pool in the same process would get less): the grid keeps one count.
-Queries that blow up in any order are left out of the sample (they measure
-the order, not the launch shapes): the sample keeps queries whose device
-time under the default choices is below --max-ms.
 """
 import argparse
 import itertools
@@ -34,15 +36,17 @@ from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
 from . import learned as L
 from . import workloads as W
 
-GRID = dict(heavy_degree=[1024, 4096], ext_blocks_per_sm=[3, 6], ext_items=[4, 8], filter_team=[8, 32],
-            step_cands=[1 << 23, 1 << 25], slots=[8])
+GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4, 8], filter_team=[8, 32],
+            step_cands=[1 << 23, 1 << 24, 1 << 25], slots=[8])
+NSLICES = 20  # the bench's slices of the batch
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="rmat22")
     ap.add_argument("--work-cap", type=int, default=5_000_000_000)
-    ap.add_argument("--queries", type=int, default=24)
+    ap.add_argument("--slices", default="0,7", help="bench slices to time (of 20)")
+    ap.add_argument("--queries", type=int, default=0, help="time this many quick queries instead")
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--max-ms", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=0, help="the slot count to tune at (0 = the grid's)")
@@ -51,16 +55,22 @@ def main():
     args = ap.parse_args()
     init(0, tuning_file=None)
     default = get_tuning()
-    wl = W.workload(args.workload, count=max(args.queries * 3, 100))
+    wl = W.workload(args.workload, count=max(args.queries * 3, 100) if args.queries else None)
     dg = DeviceGraph(wl.graph)
     model = L.load(0)
     sample = []
-    for q in wl.queries:
-        out = match(dg, q, cap=args.cap, count_only=True, order="learned", model=model, work_cap=2_000_000_000)
-        if out.info["device_ms"] < args.max_ms:
-            sample.append(q)
-        if len(sample) >= args.queries:
-            break
+    if args.queries:
+        for q in wl.queries:
+            out = match(dg, q, cap=args.cap, count_only=True, order="learned", model=model,
+                        work_cap=2_000_000_000)
+            if out.info["device_ms"] < args.max_ms:
+                sample.append(q)
+            if len(sample) >= args.queries:
+                break
+    else:
+        nq = len(wl.queries)
+        for sl in (int(x) for x in args.slices.split(",")):
+            sample.extend(wl.queries[nq * sl // NSLICES: nq * (sl + 1) // NSLICES])
     if args.slots:
         GRID["slots"] = [args.slots]
     results = []
@@ -81,7 +91,7 @@ def main():
     base = [r for r in results if all(r["choice"][k] == default.get(k, r["choice"][k]) for k in keys)]
     out = dict(choice=best["choice"], device_ms=best["device_ms"],
                default_ms=base[0]["device_ms"] if base else None, workload=args.workload,
-               sample_queries=len(sample), cap=args.cap, when=time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
+               sample_queries=len(sample), slices=None if args.queries else args.slices, cap=args.cap, when=time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
                all=results)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:

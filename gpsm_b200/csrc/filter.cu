@@ -519,9 +519,17 @@ __global__ void __launch_bounds__(256) k_cedge_count(GraphView g, const CedgeDir
     uint32_t rb, re;
     const uint32_t* cl = scan_range_team<kCedgeTeam>(g, mu, cd.lab, b, e, &rb, &re);
     uint32_t c = 0;
-    for (uint32_t j = rb + T.rank; j < re; j += kCedgeTeam) {
-      const uint32_t mv = cl[j];
-      c += (bmv[mv >> 5] >> (mv & 31)) & 1u;
+    for (uint32_t j0 = rb + T.rank; j0 < re; j0 += kScanU * kCedgeTeam) {  // kScanU loads in flight
+      uint32_t mv[kScanU];
+      bool in[kScanU];
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        in[k] = j0 + k * kCedgeTeam < re;
+        mv[k] = in[k] ? cl[j0 + k * kCedgeTeam] : 0u;
+      }
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k)
+        if (in[k]) c += (bmv[mv[k] >> 5] >> (mv[k] & 31)) & 1u;
     }
     for (int o = kCedgeTeam / 2; o > 0; o >>= 1) c += __shfl_xor_sync(T.mask, c, o);
     if (T.rank == 0) cnt[w] = c;
@@ -548,17 +556,27 @@ __global__ void __launch_bounds__(256) k_cedge_write(GraphView g, const CedgeDir
     uint32_t rb, re;
     const uint32_t* cl = scan_range_team<kCedgeTeam>(g, mu, cd.lab, b, e, &rb, &re);
     unsigned long long pos = goff[w];
-    for (uint32_t j0 = rb; j0 < re; j0 += kCedgeTeam) {
-      const uint32_t j = j0 + T.rank;
-      uint32_t mv = 0;
-      bool hit = false;
-      if (j < re) {
-        mv = cl[j];
-        hit = (bmv[mv >> 5] >> (mv & 31)) & 1u;
+    // kScanU neighbours per lane a round: their loads go out together, then
+    // they are written in adjacency order (round k covers the k-th group of
+    // kCedgeTeam neighbours)
+    for (uint32_t j0 = rb; j0 < re; j0 += kScanU * kCedgeTeam) {
+      uint32_t mv[kScanU];
+      bool hit[kScanU];
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        const uint32_t j = j0 + k * kCedgeTeam + T.rank;
+        hit[k] = j < re;
+        mv[k] = hit[k] ? cl[j] : 0u;
       }
-      const uint32_t bal = (__ballot_sync(T.mask, hit) & T.mask) >> lead;  // bit r: team rank r
-      if (hit) nbrs[pos + __popc(bal & ((1u << T.rank) - 1u))] = mv;
-      pos += __popc(bal);
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k)
+        if (hit[k]) hit[k] = (bmv[mv[k] >> 5] >> (mv[k] & 31)) & 1u;
+#pragma unroll
+      for (uint32_t k = 0; k < kScanU; ++k) {
+        const uint32_t bal = (__ballot_sync(T.mask, hit[k]) & T.mask) >> lead;  // bit r: team rank r
+        if (hit[k]) nbrs[pos + __popc(bal & ((1u << T.rank) - 1u))] = mv[k];
+        pos += __popc(bal);
+      }
     }
   }
 }

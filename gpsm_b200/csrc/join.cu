@@ -411,6 +411,7 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 
 constexpr uint32_t kWriteStage = 4096;  // words per staging buffer (two buffers)
 constexpr uint32_t kWriteRows = 1024;   // rows per chunk at most (their kept pairs are staged)
+constexpr uint32_t kWriteBlock = 256;   // threads of k_extend_write
 
 // Block per tile (grid-stride): the tile's kept rows go to output rows
 // tile_off[tile] ...; rows past out_cap are cut. Block 0 reports the rows
@@ -418,31 +419,37 @@ constexpr uint32_t kWriteRows = 1024;   // rows per chunk at most (their kept pa
 // once read, so the next step's check pass starts from zero counts.
 // The tile's output is one contiguous span. It is built in chunks of whole
 // rows in shared memory: the chunk's kept (row, value) pairs are staged
-// first (one coalesced load per row), then each thread fills one output
-// word at a time (its row by a multiply-high with the precomputed reciprocal
-// of the row width, exact for these ranges; kU input words' loads in flight
-// per thread), and the chunk leaves by one bulk copy on the async engine.
-// The chunk is laid out so that every word has the same 16-byte phase in
-// shared memory as in the output, so the aligned middle goes in one copy
-// and at most three words at each end by plain stores. Two staging buffers
-// alternate: gathering the next chunk overlaps the copy of the previous one.
-__global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
-                                                         unsigned long long row_begin, const uint2* __restrict__ kept,
-                                                         uint32_t* __restrict__ tile_cnt,
-                                                         const unsigned long long* __restrict__ tile_off,
-                                                         uint32_t ntiles_max, uint32_t ext_tile, uint32_t* __restrict__ out,
-                                                         unsigned long long out_cap, StepState* __restrict__ st,
-                                                         StepState* __restrict__ next) {
+// first (one coalesced load per row), then the threads fill the chunk in
+// row groups: thread t owns column t % w of rows t / w, t / w + g, ... (w
+// the output width, g = 256 / w rows per group), so consecutive threads
+// write consecutive words, a thread's column (an input column, or the new
+// value) never changes, and kU rows' loads are in flight per thread. The
+// chunk leaves by one bulk copy on the async engine; it is laid out so that
+// every word has the same 16-byte phase in shared memory as in the output,
+// so the aligned middle goes in one copy and at most three words at each
+// end by plain stores. Two staging buffers alternate: gathering the next
+// chunk overlaps the copy of the previous one.
+__global__ void __launch_bounds__(kWriteBlock, 4) k_extend_write(const uint32_t* __restrict__ in, uint32_t cols,
+                                                                 unsigned long long row_begin,
+                                                                 const uint2* __restrict__ kept,
+                                                                 uint32_t* __restrict__ tile_cnt,
+                                                                 const unsigned long long* __restrict__ tile_off,
+                                                                 uint32_t ntiles_max, uint32_t ext_tile,
+                                                                 uint32_t* __restrict__ out,
+                                                                 unsigned long long out_cap,
+                                                                 StepState* __restrict__ st,
+                                                                 StepState* __restrict__ next) {
   constexpr int kU = 4;
   __shared__ __align__(128) uint32_t sbuf[2][kWriteStage + 4];
   __shared__ uint2 s_kept[kWriteRows];
-  const uint32_t out_cols = cols + 1;
+  const uint32_t out_cols = cols + 1;  // at most 128
   // >= 31 rows (rows hold at most 128 words), <= kWriteRows
   const uint32_t chunk_rows = min(kWriteStage / out_cols, kWriteRows);
-  // ceil(2^32 / out_cols): __umulhi(k, recip) == k / out_cols for every
-  // k < 2^32 / out_cols (here k < kWriteStage)
-  const uint32_t recip = (uint32_t)((0x100000000ull + out_cols - 1) / out_cols);
-  const uint32_t* __restrict__ inb = in + row_begin * cols;  // row r of this step: inb + r * cols
+  const uint32_t group = kWriteBlock / out_cols;  // rows per group, >= 2
+  const uint32_t trow = threadIdx.x / out_cols, tcol = threadIdx.x - trow * out_cols;
+  const bool gathers = trow < group;  // threads past the last whole row of a group idle
+  const bool new_col = tcol == cols;  // this thread writes the new value
+  const uint32_t* __restrict__ inb = in + row_begin * cols + tcol;  // column tcol of row r: inb + r * cols
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->written = min(tile_off[ntiles_max], out_cap);
     *next = StepState{};  // the next step starts from zero
@@ -464,25 +471,22 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
       uint32_t* sb = sbuf[chunk_no & 1];
       if (threadIdx.x == 0) bulk_wait_read<1>();  // the copy that last read this buffer is done with it
       __syncthreads();  // ... and the previous chunk's gather no longer reads s_kept
-      for (uint32_t i = threadIdx.x; i < nq; i += blockDim.x) s_kept[i] = __ldg(kt + q0 + i);
+      for (uint32_t i = threadIdx.x; i < nq; i += kWriteBlock) s_kept[i] = __ldg(kt + q0 + i);
       __syncthreads();
-      for (uint32_t kb = threadIdx.x; kb < words; kb += kU * blockDim.x) {
-        uint32_t col[kU], val[kU];
-        uint2 e[kU];
+      if (gathers) {
+        uint32_t* sw = sb + lead + threadIdx.x;  // word (trow, tcol) of the chunk; a group is group*w words
+        for (uint32_t r0 = trow; r0 < nq; r0 += kU * group, sw += kU * group * out_cols) {
+          uint32_t val[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const uint32_t k = kb + u * blockDim.x;
-          const uint32_t q = __umulhi(k, recip);
-          col[u] = k - q * out_cols;
-          e[u] = k < words ? s_kept[q] : make_uint2(0u, 0u);
+          for (int u = 0; u < kU; ++u) {
+            const uint32_t r = r0 + u * group;
+            const uint2 e = r < nq ? s_kept[r] : make_uint2(0u, 0u);
+            val[u] = (r < nq && !new_col) ? __ldg(inb + (size_t)e.x * cols) : e.y;
+          }
+#pragma unroll
+          for (int u = 0; u < kU; ++u)
+            if (r0 + u * group < nq) sw[u * group * out_cols] = val[u];
         }
-#pragma unroll
-        for (int u = 0; u < kU; ++u)
-          val[u] = (kb + u * blockDim.x < words && col[u] < cols) ? __ldg(inb + (size_t)e[u].x * cols + col[u])
-                                                                  : e[u].y;
-#pragma unroll
-        for (int u = 0; u < kU; ++u)
-          if (kb + u * blockDim.x < words) sb[lead + kb + u * blockDim.x] = val[u];
       }
       proxy_fence_shared();
       __syncthreads();
@@ -501,7 +505,7 @@ __global__ void __launch_bounds__(256, 4) k_extend_write(const uint32_t* __restr
         if (t < k0) dst[t] = sb[lead + t];
         else if (t >= 4 && t - 4 < words - k1) dst[k1 + t - 4] = sb[lead + k1 + t - 4];
       } else {
-        for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) dst[k] = sb[lead + k];
+        for (uint32_t k = threadIdx.x; k < words; k += kWriteBlock) dst[k] = sb[lead + k];
       }
     }
   }
@@ -580,6 +584,10 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
     set_last_error("join step: misaligned row buffer");
     throw CudaError{cudaErrorInvalidValue, "join alignment"};
   }
+  if (in_cols + 1 > 128) {  // the write pass puts at least two rows in a 256-thread group
+    set_last_error("join step: rows wider than 128 words");
+    throw CudaError{cudaErrorInvalidValue, "join width"};
+  }
   const uint64_t ltiles = (nrows + kLocBlock - 1) / kLocBlock;
   Lookback lb1 = next_lb(ws, ltiles);
   k_locate<<<(uint32_t)ltiles, kLocBlock, 0, ws.stream>>>(in, in_cols, row_begin, nrows, d_back, nb, nbrs_total,
@@ -599,7 +607,7 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   GPSM_LAUNCHED();
   launch_scan_u32(ws, js.tile_cnt, std::max<uint64_t>(ntiles_max, 1), js.tile_off);
   const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));
-  k_extend_write<<<wgrid, 256, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
+  k_extend_write<<<wgrid, kWriteBlock, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
                                                (uint32_t)std::max<uint64_t>(ntiles_max, 1), ext_tile, out, out_cap,
                                                d_st, d_next);
   GPSM_LAUNCHED();

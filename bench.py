@@ -366,6 +366,7 @@ def run_ours(args):
     except G.GpsmError as ex:
         e2e_err = str(ex)
     barrier(pg)
+    pool0 = G.host_pool_stats()
     t1 = time.perf_counter()
     if e2e_err is None:
         try:
@@ -379,6 +380,7 @@ def run_ours(args):
         except G.GpsmError as ex:
             e2e_err = str(ex)
     e2e_wall = max_over_ranks(pg, time.perf_counter() - t1)
+    pool1 = G.host_pool_stats()
     if srv is not None:
         try:
             srv.close()
@@ -464,7 +466,10 @@ def run_ours(args):
                      "d2h_bytes_per_step": int(e2e_d2h / max(world, 1)), "rows_per_s": e2e_rows / e2e_wall,
                      "d2h_gb_per_s": e2e_d2h / 1e9 / e2e_wall,
                      "basis": "request server, slice 0 (host query arrays in, every embedding row to host "
-                              "memory, results taken as they finish), after one untimed pass"}),
+                              "memory, results taken as they finish), after one untimed pass",
+                     "host_pool": {"blocks": pool1["blocks"], "pinned_gb": pool1["pinned_bytes"] / 1e9,
+                                   "grown_in_timed_pass": pool1["grown"] - pool0["grown"],
+                                   "grow_ms_in_timed_pass": pool1["grow_ms"] - pool0["grow_ms"]}}),
             "gpu_launches": int(sum_over_ranks(pg, tot["launches"])),
             "clocks": clk,
             "wall_s": wall,

@@ -20,7 +20,7 @@ from . import _lib
 from ._lib import GpsmError  # noqa: F401
 
 __all__ = ["init", "shutdown", "DeviceGraph", "Engine", "match", "match_batch", "flush_l2", "MatchOutput",
-           "debug_filter", "GpsmError", "pack_queries", "Model", "order_features", "last_levels", "Server",
+           "debug_filter", "GpsmError", "pack_queries", "Model", "order_features", "last_levels", "Server", "host_pool_stats",
            "set_tuning", "get_tuning"]
 
 
@@ -377,6 +377,15 @@ def last_levels(n, engine=None):
     eng = engine.handle if engine is not None else None
     _lib.check(lib.gpsm_last_levels(eng, n, _lib.ptr(a), _lib.ptr(b), _lib.ptr(c)), "gpsm_last_levels")
     return a, b, c
+
+
+def host_pool_stats():
+    """The page-locked result-block pool: blocks held, bytes pinned, blocks
+    added since the process started and the host ms spent pinning them."""
+    lib = _lib.load()
+    v = [C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_double()]
+    lib.gpsm_host_pool_stats(*[C.byref(x) for x in v])
+    return dict(blocks=v[0].value, pinned_bytes=v[1].value, grown=v[2].value, grow_ms=v[3].value)
 
 
 class Server:

@@ -65,6 +65,7 @@ SIGNATURES = {
     "gpsm_engine_match": (C.c_int, [vp, vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]),
     "gpsm_match": (C.c_int, [vp, u32, vp, u32, vp, u64, vp, vp, vp, vp]),
     "gpsm_free": (None, [vp]),
+    "gpsm_host_pool_stats": (None, [vp, vp, vp, vp]),
     "gpsm_debug_filter": (C.c_int, [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_match_batch": (C.c_int, [vp, vp, u32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "gpsm_flush_l2": (C.c_int, [vp, u64]),

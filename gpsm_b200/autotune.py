@@ -12,7 +12,7 @@ after a warm-up) under every combination of:
   ext_items          candidates per thread of the join-check kernel (4 or 8:
                      its tile is 256 x ext_items candidates; a thread keeps
                      one row's state and list positions across its items)
-  filter_team        lanes per candidate in the refinement steps (8 or 32)
+  filter_team        lanes per candidate in the refinement steps (4, 8 or 32)
   step_cands         candidates one join step may admit
   slots              engine slots running queries at once
 and writes the fastest combination to --out; gpsm_b200.init() applies it.
@@ -36,8 +36,8 @@ from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
 from . import learned as L
 from . import workloads as W
 
-GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4, 8], filter_team=[8, 32],
-            step_cands=[1 << 23, 1 << 24, 1 << 25], slots=[8])
+GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4], filter_team=[4, 8, 32],
+            step_cands=[1 << 23, 1 << 24], slots=[8])
 NSLICES = 20  # the bench's slices of the batch
 
 

@@ -327,6 +327,10 @@ int gpsm_match(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t q
 
 void gpsm_free(void* p) { host_free(p); }
 
+void gpsm_host_pool_stats(uint64_t* blocks, uint64_t* pinned_bytes, uint64_t* grown, double* grow_ms) {
+  host_pool_stats(blocks, pinned_bytes, grown, grow_ms);
+}
+
 int gpsm_last_levels(gpsm_engine_t eng, uint32_t n, uint64_t* level_in, uint64_t* level_cands, uint64_t* level_out) {
   gpsm_engine_s* e = engine_or_default(eng);
   if (!e) return GPSM_ERR_STATE;

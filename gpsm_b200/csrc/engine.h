@@ -160,6 +160,7 @@ class HostRows {
 
 // Frees a result block: back to the pool if it came from there, else free().
 void host_free(void* p);
+void host_pool_stats(uint64_t* blocks, uint64_t* pinned_bytes, uint64_t* grown, double* grow_ms);
 
 struct MatchResult {
   uint64_t rows = 0;

@@ -3,7 +3,9 @@
 // A capped query of 10^7 rows and 12 columns returns 480 MB; a serving loop
 // returns one such block per request. Two paths:
 //
-// Pooled (the usual one): a process-wide pool of page-locked blocks. A query
+// Pooled (the usual one): a process-wide pool of page-locked blocks (malloc'd
+// memory registered with the driver, or cudaHostAlloc memory when
+// GPSM_HOST_POOL_ALLOC=hostalloc). A query
 // with an embedding cap takes a block large enough for cap rows before its
 // joins start; the device copies rows straight into it (one DMA per flush,
 // no bounce copy, no page faults: the block was touched and pinned when the
@@ -22,6 +24,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -40,7 +43,13 @@ struct HostPool {
   std::unordered_map<void*, uint64_t> owned;   // every pool block -> capacity bytes
   uint64_t pinned = 0;
   uint64_t limit = 0;
+  uint64_t grown = 0;     // blocks added since the process started
+  double grow_ms = 0;     // host time spent touching and pinning them
+  // blocks from cudaHostAlloc instead of malloc'd memory registered with
+  // cudaHostRegister (GPSM_HOST_POOL_ALLOC=hostalloc)
+  bool host_alloc = false;
   HostPool() {
+    if (const char* a = getenv("GPSM_HOST_POOL_ALLOC")) host_alloc = strcmp(a, "hostalloc") == 0;
     if (const char* e = getenv("GPSM_HOST_POOL_GB")) {
       limit = (uint64_t)(atof(e) * (double)(1ull << 30));
     } else {
@@ -76,15 +85,22 @@ void* pool_acquire(uint64_t bytes, uint64_t* cap) {
     if (P.pinned + size > P.limit) return nullptr;
     P.pinned += size;
   }
+  const auto t0 = std::chrono::steady_clock::now();
   void* b = nullptr;
-  bool ok = posix_memalign(&b, 2ull << 20, size) == 0;
-  if (ok) {
-    madvise(b, size, MADV_HUGEPAGE);
-    memset(b, 0, size);  // fault the pages in now, once
-    ok = cudaHostRegister(b, size, cudaHostRegisterDefault) == cudaSuccess;
-    if (!ok) {
-      cudaGetLastError();
-      free(b);
+  bool ok;
+  if (P.host_alloc) {
+    ok = cudaHostAlloc(&b, size, cudaHostAllocDefault) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+  } else {
+    ok = posix_memalign(&b, 2ull << 20, size) == 0;
+    if (ok) {
+      madvise(b, size, MADV_HUGEPAGE);
+      memset(b, 0, size);  // fault the pages in now, once
+      ok = cudaHostRegister(b, size, cudaHostRegisterDefault) == cudaSuccess;
+      if (!ok) {
+        cudaGetLastError();
+        free(b);
+      }
     }
   }
   std::lock_guard<std::mutex> lk(P.mu);
@@ -93,11 +109,22 @@ void* pool_acquire(uint64_t bytes, uint64_t* cap) {
     return nullptr;
   }
   P.owned[b] = size;
+  ++P.grown;
+  P.grow_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   *cap = size;
   return b;
 }
 
 }  // namespace
+
+void host_pool_stats(uint64_t* blocks, uint64_t* pinned_bytes, uint64_t* grown, double* grow_ms) {
+  HostPool& P = pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  if (blocks) *blocks = P.owned.size();
+  if (pinned_bytes) *pinned_bytes = P.pinned;
+  if (grown) *grown = P.grown;
+  if (grow_ms) *grow_ms = P.grow_ms;
+}
 
 bool host_pool_release(void* p) {
   if (!p) return false;

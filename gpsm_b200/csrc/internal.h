@@ -42,6 +42,10 @@ enum DeviceFlag : uint32_t {
   DF_BOUNDS = 1u << 2,      // an index check failed (result invalid)
   DF_OVERFLOW = 1u << 3,    // a 32-bit count overflowed
 };
+// Workspace::d_flags[kFilterCtr], [kFilterCtr + 1]: the filter steps' chunk
+// counter and finished-warp count (zero between launches; the flags are
+// cleared at the start of every query)
+constexpr uint32_t kFilterCtr = 32;
 
 // ---------------------------------------------------------------------------
 // device-resident data graph (uploaded once, reused by every query)
@@ -142,7 +146,7 @@ struct Workspace {
   cudaStream_t stream = nullptr;
   Arena arena;
   ScanState scan;
-  uint32_t* d_flags = nullptr;      // [16] device flags and small counters
+  uint32_t* d_flags = nullptr;      // [64] device flags and small counters
   unsigned long long* d_small = nullptr;  // [64] device scratch for results of scans
   unsigned long long* h_small = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, evm = nullptr, ev1 = nullptr;

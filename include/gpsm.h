@@ -197,6 +197,10 @@ int gpsm_match(gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t q
                const uint32_t* q_edges, uint64_t cap, uint32_t** out_rows, uint64_t* out_nrows,
                uint32_t* out_ncols, int32_t* id_map);
 void gpsm_free(void* p);
+/* The process-wide pool of page-locked result blocks: blocks it holds,
+ * bytes pinned, blocks added since the process started and the host time
+ * spent touching and pinning them (no counterpart in the reference). */
+void gpsm_host_pool_stats(uint64_t* blocks, uint64_t* pinned_bytes, uint64_t* grown, double* grow_ms);
 
 /* Matches nq queries back to back (query k: labels q_labels[q_voff[k]..],
  * edges q_edges[2*q_eoff[k]..]); rows are produced in device memory and
@@ -307,7 +311,7 @@ typedef struct gpsm_tuning {
   uint64_t race_share;         /* learned order: first work share (candidates) when the learned plan
                                   and the plain order take turns (default 2^28) */
   uint32_t ext_items;          /* candidates per thread of the join check kernel: 4 or 8 (default 4) */
-  uint32_t filter_team;        /* lanes per candidate in the refinement steps: 8 or 32 (default 8) */
+  uint32_t filter_team;        /* lanes per candidate in the refinement steps: 4, 8 or 32 (default 8) */
 } gpsm_tuning;
 int gpsm_set_tuning(const gpsm_tuning* t);
 int gpsm_get_tuning(gpsm_tuning* t);

@@ -358,7 +358,7 @@ def run_ours(args):
     try:
         srv = G.Server(dg, slots=slots, cap=cap, order=args.order if args.order == "learned" else None,
                        model=model, collect_rows=True, work_cap=work_cap,
-                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)) >> 21 << 21)
+                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)) >> 21 << 21, largest_first=True)
         for q in e2e_qs:  # untimed: grows the pool of page-locked result blocks
             srv.submit(q)
         for _ in e2e_qs:
@@ -465,8 +465,9 @@ def run_ours(args):
                     {"value": e2e_q / e2e_wall, "unit": "queries/s", "h2d_bytes_per_step": h2d,
                      "d2h_bytes_per_step": int(e2e_d2h / max(world, 1)), "rows_per_s": e2e_rows / e2e_wall,
                      "d2h_gb_per_s": e2e_d2h / 1e9 / e2e_wall,
-                     "basis": "request server, slice 0 (host query arrays in, every embedding row to host "
-                              "memory, results taken as they finish), after one untimed pass",
+                     "basis": "request server, slice 0 submitted at once (host query arrays in, every embedding "
+                              "row to host memory, largest request first, results taken as they finish), after "
+                              "one untimed pass",
                      "host_pool": {"blocks": pool1["blocks"], "pinned_gb": pool1["pinned_bytes"] / 1e9,
                                    "grown_in_timed_pass": pool1["grown"] - pool0["grown"],
                                    "grow_ms_in_timed_pass": pool1["grow_ms"] - pool0["grow_ms"]}}),

@@ -394,13 +394,15 @@ class Server:
     joins when their predicted join memory fits memory_budget bytes."""
 
     def __init__(self, dgraph, slots=4, memory_budget=0, slot_arena=0, cap=None, order=None, model=None,
-                 collect_rows=False, work_cap=0, result_rows=0):
+                 collect_rows=False, work_cap=0, result_rows=0, largest_first=False):
         lib = _lib.load()
         self._lib = lib
         opts = _lib.MatchOpts()
         opts.cap = int(cap or 0)
         opts.work_cap = int(work_cap)
         opts.result_rows = int(result_rows)  # device rows per copy to the host (0: 4 Mi)
+        if largest_first:  # a free slot takes the queued request with the most edges
+            opts.flags |= _lib.GPSM_F_LARGEST_FIRST
         if order == "learned":
             opts.order_mode = _lib.GPSM_ORDER_LEARNED
             opts.model = model.handle

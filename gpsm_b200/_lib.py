@@ -94,7 +94,7 @@ SIGNATURES = {
 }
 
 GPSM_ORDER_PLAIN, GPSM_ORDER_GIVEN, GPSM_ORDER_LEARNED = 0, 1, 2
-GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE, GPSM_F_DIRECTED = 1, 2, 4
+GPSM_F_COUNT_ONLY, GPSM_F_KEEP_ON_DEVICE, GPSM_F_DIRECTED, GPSM_F_LARGEST_FIRST = 1, 2, 4, 8
 
 
 class MatchOpts(C.Structure):

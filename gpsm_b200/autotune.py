@@ -20,6 +20,8 @@ Whole slices keep the queries that run to the work cap: they decide the
 step budget (a budget whose scratch outgrows L2 slows every long query) and
 a sample of quick queries alone picked the wrong one. --queries N instead
 times N quick queries (device time under --max-ms each).
+The grid keeps what earlier sweeps left open (a 4,096 hub threshold, 6
+check blocks per SM and 4 candidates per check thread won every sweep).
 Slot counts are compared one process each (--slots; a process sizes every
 slot pool from the memory left free when the pool is created, so a second
 pool in the same process would get less): the grid keeps one count.

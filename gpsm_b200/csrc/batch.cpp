@@ -215,7 +215,21 @@ struct Server {
   uint32_t active = 0;
   MatchOptions base;
   bool collect = false;
+  bool largest_first = false;  // GPSM_F_LARGEST_FIRST
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+  // The next request for a free slot (mu held, queue not empty): the oldest,
+  // or with largest_first the one with the most query edges, then vertices
+  // (a long request started early does not run alone at the end).
+  Request* take_next() {
+    auto pick = queue.begin();
+    if (largest_first)
+      for (auto it = queue.begin(); it != queue.end(); ++it)
+        if ((*it)->qm > (*pick)->qm || ((*it)->qm == (*pick)->qm && (*it)->qn > (*pick)->qn)) pick = it;
+    Request* r = *pick;
+    queue.erase(pick);
+    return r;
+  }
 
   double now_ms() const {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -255,8 +269,7 @@ struct Server {
         std::unique_lock<std::mutex> lk(mu);
         cv_q.wait(lk, [&] { return stopping || !queue.empty(); });
         if (queue.empty()) return;  // stopping and drained
-        r = queue.front();
-        queue.pop_front();
+        r = take_next();
         ++active;
         r->t_start = now_ms();
       }
@@ -407,6 +420,7 @@ int gpsm_server_create(gpsm_graph_t g, uint32_t slots, uint64_t memory_budget, u
     S->g = g->g;
     S->base = options_from(opts);
     S->collect = collect_rows != 0;
+    S->largest_first = opts && (opts->flags & GPSM_F_LARGEST_FIRST) != 0;
     S->base.keep_on_device = !S->collect;
     if (!S->collect && S->base.cap != ~0ULL) S->base.result_rows = std::max<uint64_t>(S->base.result_rows, S->base.cap);
     const uint64_t arena = slot_arena_bytes(slots, slot_arena);

@@ -417,33 +417,24 @@ __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint3
                                                      uint32_t light_blocks, uint32_t cw, uint32_t u,
                                                      const uint32_t* __restrict__ tgt, uint32_t ntgt,
                                                      uint32_t* __restrict__ bm, uint32_t words,
-                                                     const uint32_t* __restrict__ flags, uint32_t* __restrict__ ctr,
-                                                     RefineStamp rs) {
+                                                     const uint32_t* __restrict__ flags, RefineStamp rs) {
   constexpr uint32_t kStride = EXPLORE ? 3 : 2;
   constexpr uint32_t kTeam = TEAM;
   extern __shared__ uint32_t s_tgt[];
   __shared__ uint32_t s_chunk[8][32 * 32];  // per warp: the candidates of one chunk (at most 32 words)
   for (uint32_t i = threadIdx.x; i < kStride * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
-  // both exits below hold for the whole launch, so either every light warp
-  // takes chunks (and counts itself out at the end) or none does
   if (*flags & DF_EMPTY) return;
   if (!EXPLORE && refine_is_noop(rs, s_tgt, ntgt)) return;
   uint32_t* bmu = bm + (size_t)u * words;
   if (blockIdx.x < light_blocks) {
-    // each warp takes chunks of cw bitmap words from a counter (ctr[0]) until
-    // they run out, so a warp that drew busy chunks does not hold the launch
-    // up while the others idle; it lists a chunk's candidates (ascending) in
-    // shared memory, then its 32 / TEAM teams take them in turn
+    // each warp lists its chunk's candidates (ascending) in shared memory,
+    // then its four 8-lane teams take them in turn: four candidates' chains
+    // of dependent loads in flight per warp instead of one
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nchunks = (words + cw - 1) / cw;
+    const uint32_t nwarps = light_blocks * (blockDim.x >> 5);
     uint32_t* wl = s_chunk[threadIdx.x >> 5];
-    for (;;) {
-      uint32_t ci = 0;
-      if (lane == 0) ci = atomicAdd(&ctr[0], 1u);
-      ci = __shfl_sync(0xffffffffu, ci, 0);
-      if (ci >= nchunks) break;
-      const uint32_t c0 = ci * cw;
+    for (uint32_t c0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * cw; c0 < words; c0 += nwarps * cw) {
       // each word of the chunk belongs to this warp alone: only its own
       // candidates' bits are cleared while it runs
       const uint32_t wv = (lane < cw && c0 + lane < words) ? bmu[c0 + lane] : 0u;
@@ -467,15 +458,6 @@ __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint3
         else refine_one<kTeam>(g, mu, b, e, s_tgt, ntgt, bm, words, bmu, rs, u);
       }
       __syncwarp();  // the list is rewritten for the next chunk
-    }
-    // the last light warp out resets the counters for the next launch on
-    // this stream (they start the query at zero)
-    if (lane == 0) {
-      __threadfence();
-      if (atomicAdd(&ctr[1], 1u) == light_blocks * (blockDim.x >> 5) - 1) {
-        ctr[0] = 0;
-        ctr[1] = 0;
-      }
     }
     return;
   }
@@ -792,19 +774,15 @@ static HeavyList heavy_list(Workspace& ws, const DeviceGraph& g) {
   return hl;
 }
 
-// Words per warp chunk of a bitmap of `words` words: about 32768 chunks
-// (several per resident warp, so the warps that drew busy chunks are
-// balanced by the others taking more), at most 32 words (one per lane).
-static uint32_t chunk_words(uint32_t words) {
-  return std::max<uint32_t>(1, std::min<uint32_t>(32, (words + 32767) / 32768));
-}
+// Words per warp chunk of a bitmap of `words` words: about 8192 warps (a
+// full B200 holds 148 x 64), at most 32 words (one per lane) a chunk.
+static uint32_t chunk_words(uint32_t words) { return std::max<uint32_t>(1, std::min<uint32_t>(32, (words + 8191) / 8192)); }
 
-// Blocks of 8 warps taking the chunks: one per chunk group of 8 when there
-// are few, else as many as the SMs hold at once (4 per SM).
+// Blocks of 8 warps that cover the bitmap in chunks of chunk_words(words).
 static uint32_t light_blocks_for(uint32_t words) {
   const uint32_t cw = chunk_words(words);
   const uint32_t chunks = (words + cw - 1) / cw;
-  return std::max<uint32_t>(1, std::min<uint32_t>((chunks + 7) / 8, (uint32_t)sm_count() * 4));
+  return std::max<uint32_t>(1, std::min<uint32_t>((chunks + 7) / 8, 148 * 16));
 }
 
 template <bool EXPLORE>
@@ -822,13 +800,13 @@ static void launch_filter_step(Workspace& ws, const DeviceGraph& g, uint32_t u, 
   const uint32_t team = tuning().filter_team;
   if (EXPLORE || team >= 32)
     k_filter_step<EXPLORE, 32><<<light + hubs, 256, smem, ws.stream>>>(
-        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, ws.d_flags + kFilterCtr, rs);
+        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
   else if (team <= 4)
     k_filter_step<false, 4><<<light + hubs, 256, smem, ws.stream>>>(
-        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, ws.d_flags + kFilterCtr, rs);
+        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
   else
     k_filter_step<false, 8><<<light + hubs, 256, smem, ws.stream>>>(
-        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, ws.d_flags + kFilterCtr, rs);
+        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
   GPSM_LAUNCHED();
 }
 

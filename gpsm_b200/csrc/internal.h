@@ -42,10 +42,6 @@ enum DeviceFlag : uint32_t {
   DF_BOUNDS = 1u << 2,      // an index check failed (result invalid)
   DF_OVERFLOW = 1u << 3,    // a 32-bit count overflowed
 };
-// Workspace::d_flags[kFilterCtr], [kFilterCtr + 1]: the filter steps' chunk
-// counter and finished-warp count (zero between launches; the flags are
-// cleared at the start of every query)
-constexpr uint32_t kFilterCtr = 32;
 
 // ---------------------------------------------------------------------------
 // device-resident data graph (uploaded once, reused by every query)

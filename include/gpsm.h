@@ -125,6 +125,9 @@ typedef struct gpsm_model_s* gpsm_model_t; /* learned join-order model (MLP on o
 #define GPSM_F_DIRECTED 4u        /* keep rows whose query edges a->b (label) are data edges
                                      row[a]->row[b] with that label: IO::verify on the device
                                      (io/IO.cpp:146-180); needs gpsm_graph_set_directed */
+#define GPSM_F_LARGEST_FIRST 8u   /* gpsm_server_create: a free slot takes the queued request
+                                     with the most query edges (then vertices) instead of the
+                                     oldest; ties in submission order */
 
 typedef struct gpsm_match_opts {
   uint64_t cap;          /* embedding cap: stop after the first `cap` rows; 0 = none */

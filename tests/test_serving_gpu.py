@@ -118,3 +118,18 @@ def test_rows_copied_while_the_slot_moves_on(gpu, mixed):
         assert r["status"] == 0 and r["rows"] == ref.count
         assert np.array_equal(r["table"][:, r["id_map"]], ref.embeddings())
     srv.close()
+
+
+def test_largest_first_serves_the_biggest_queued_request_next(gpu, mixed):
+    """With GPSM_F_LARGEST_FIRST a free slot takes the queued request with
+    the most query edges (then vertices): on one slot, every request after
+    the first to start ran in non-increasing (edges, vertices) order."""
+    g, qs, dg = mixed
+    srv = gpu.Server(dg, slots=1, cap=1000, largest_first=True)
+    tickets = {srv.submit(q): q for q in qs[:12]}
+    infos = {t: srv.wait(t) for t in tickets}
+    srv.close()
+    started = sorted(tickets, key=lambda t: infos[t]["start_ms"])
+    keys = [(tickets[t].m, tickets[t].n) for t in started[1:]]
+    assert all(a >= b for a, b in zip(keys, keys[1:])), keys
+    assert len(set(keys)) > 1

@@ -352,8 +352,10 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   GPSM_CUDA(cudaMemcpyAsync(d_fixed, plain.data(), Q.n * 4, cudaMemcpyHostToDevice, s));
   launch_plan(s, opt.model, d_q, d_e, d_st, (uint32_t)starts.size(), d_fixed, d_out);
   std::vector<char> hout(plan_out_bytes() * (starts.size() + 1));
-  GPSM_CUDA(cudaMemcpyAsync(hout.data(), d_out, hout.size(), cudaMemcpyDeviceToHost, s));
+  char* h_plan = reinterpret_cast<char*>(ws.h_small + 2048);  // the plans, through the pinned mirror
+  small_to_host(ws, h_plan, d_out, hout.size());
   GPSM_CUDA(cudaStreamSynchronize(s));
+  memcpy(hout.data(), h_plan, hout.size());
   ws.arena.used = mark;  // planner scratch is not needed by the joins
   const size_t ob = plan_out_bytes();
   int best = -1;
@@ -541,8 +543,8 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
   // ---- final candidate lists with ranks (one launch for every vertex) ------
   launch_compact_multi(ws, bm, W, qn, d_lists, rank, counts);
   ++launches;
-  GPSM_CUDA(cudaMemcpyAsync(ws.h_small, counts, qn * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-  GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 64, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  small_to_host(ws, ws.h_small, counts, qn * sizeof(uint32_t));
+  small_to_host(ws, ws.h_small + 64, ws.d_flags, sizeof(uint32_t));
   GPSM_CUDA(cudaStreamSynchronize(s));
   std::vector<uint32_t> cnt(qn);
   memcpy(cnt.data(), ws.h_small, qn * sizeof(uint32_t));
@@ -599,9 +601,8 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
     launch_cedge_count(ws, g, d_dirs, ndir, d_idx, items, bm, ccount);
     launch_scan_u32(ws, ccount, items, goff);
     launch_gather_u64(ws, goff, d_idx, ndir + 1, ws.d_small);
-    GPSM_CUDA(cudaMemcpyAsync(ws.h_small, ws.d_small, (ndir + 1) * sizeof(unsigned long long),
-                              cudaMemcpyDeviceToHost, s));
-    GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4000, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    small_to_host(ws, ws.h_small, ws.d_small, (ndir + 1) * sizeof(unsigned long long));
+    small_to_host(ws, ws.h_small + 4000, ws.d_flags, sizeof(uint32_t));
     GPSM_CUDA(cudaStreamSynchronize(s));
     if (*reinterpret_cast<uint32_t*>(ws.h_small + 4000) & DF_SCAN_TIMEOUT) {
       set_last_error("device wait limit tripped in candidate-edge scan");
@@ -974,7 +975,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 4;  // locate, check, scan, write
     ++R.stats.join_steps;
-    GPSM_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(StepState), cudaMemcpyDeviceToHost, s));
+    small_to_host(ws, h_st, d_st, sizeof(StepState));
     GPSM_CUDA(cudaStreamSynchronize(s));
     {
       float ems = 0;
@@ -1012,7 +1013,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     if (final_level && opt.directed && written) {
       launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
                              res_buf + res_used * qn, d_kept);
-      GPSM_CUDA(cudaMemcpyAsync(&h_st->verified, d_kept, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+      small_to_host(ws, &h_st->verified, d_kept, sizeof(unsigned long long));
       GPSM_CUDA(cudaStreamSynchronize(s));
       kept = std::min<uint64_t>(h_st->verified, cap - emitted);  // the cap counts rows that pass
       ++exp_launches;
@@ -1198,7 +1199,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   R.stats.expand_launches = ctx.exp_launches;
   R.stats.alg_bytes_join = ctx.alg_bytes;
   if (jrc != GPSM_OK) return jrc;
-  GPSM_CUDA(cudaMemcpyAsync(ws.h_small + 4001, ws.d_flags, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  small_to_host(ws, ws.h_small + 4001, ws.d_flags, sizeof(uint32_t));
   GPSM_CUDA(cudaEventSynchronize(ws.ev1));
   GPSM_CUDA(cudaStreamSynchronize(s));
   if (*reinterpret_cast<uint32_t*>(ws.h_small + 4001) & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {

@@ -395,12 +395,23 @@ __device__ __forceinline__ void refine_one(const GraphView& g, uint32_t mu, uint
   }
 }
 
-// True when no target's candidate set changed since u's previous refinement.
-__device__ __forceinline__ bool refine_is_noop(const RefineStamp& rs, const uint32_t* tgt, uint32_t ntgt) {
-  if (rs.prev == 0) return false;
+// Refinement targets worth checking, compacted in place in shared memory
+// (thread 0; the caller syncs): every candidate left in C(u) had a
+// neighbour in each target's set when u was last refined, and a set only
+// shrinks, so a target whose set has not changed since u's previous
+// refinement (its stamp is older) cannot reject anyone. Skipping it leaves
+// the sets exactly those of checking every target. All of them on u's first
+// refinement.
+__device__ __forceinline__ uint32_t refine_targets(const RefineStamp& rs, uint32_t* tgt, uint32_t ntgt) {
+  if (rs.prev == 0) return ntgt;
+  uint32_t n = 0;
   for (uint32_t t = 0; t < ntgt; ++t)
-    if (rs.stamp[tgt[2 * t]] >= rs.prev) return false;
-  return true;
+    if (rs.stamp[tgt[2 * t]] >= rs.prev) {
+      tgt[2 * n] = tgt[2 * t];
+      tgt[2 * n + 1] = tgt[2 * t + 1];
+      ++n;
+    }
+  return n;
 }
 
 // EXPLORE: explore_one; otherwise refine_one. hubs: [hub_begin, hub_end) of
@@ -422,10 +433,18 @@ __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint3
   constexpr uint32_t kTeam = TEAM;
   extern __shared__ uint32_t s_tgt[];
   __shared__ uint32_t s_chunk[8][32 * 32];  // per warp: the candidates of one chunk (at most 32 words)
+  __shared__ uint32_t s_ntgt;
   for (uint32_t i = threadIdx.x; i < kStride * ntgt; i += blockDim.x) s_tgt[i] = tgt[i];
   __syncthreads();
   if (*flags & DF_EMPTY) return;
-  if (!EXPLORE && refine_is_noop(rs, s_tgt, ntgt)) return;
+  if (!EXPLORE) {
+    // only targets whose sets changed since u's previous refinement (the
+    // stamps do not change during the launch: it stamps u alone)
+    if (threadIdx.x == 0) s_ntgt = refine_targets(rs, s_tgt, ntgt);
+    __syncthreads();
+    ntgt = s_ntgt;
+    if (ntgt == 0) return;  // nothing can change
+  }
   uint32_t* bmu = bm + (size_t)u * words;
   if (blockIdx.x < light_blocks) {
     // each warp lists its chunk's candidates (ascending) in shared memory,
@@ -737,6 +756,28 @@ static uint32_t grid_for(uint64_t warps_needed, uint32_t cap_blocks) {
   if (blocks < 1) blocks = 1;
   if (blocks > cap_blocks) blocks = cap_blocks;
   return (uint32_t)blocks;
+}
+
+// Small device results to the workspace's page-locked mirror: one block
+// stores the words into the mirror through its device address and fences
+// them to the system, so the host reads them after a stream sync.
+__global__ void k_words_to_host(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t n) {
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  __threadfence_system();
+}
+
+void small_to_host(Workspace& ws, void* h_dst, const void* d_src, size_t bytes) {
+  const size_t off = (size_t)((const char*)h_dst - (const char*)ws.h_small);
+  if (bytes == 0) return;
+  if ((const char*)h_dst < (const char*)ws.h_small || off + bytes > 4096 * sizeof(unsigned long long) ||
+      (off | bytes | (size_t)(uintptr_t)d_src) & 3) {
+    set_last_error("small_to_host: destination outside the mirror or unaligned");
+    throw CudaError{cudaErrorInvalidValue, "small_to_host"};
+  }
+  k_words_to_host<<<1, 256, 0, ws.stream>>>(static_cast<const uint32_t*>(d_src),
+                                            reinterpret_cast<uint32_t*>((char*)ws.h_small_dev + off),
+                                            (uint32_t)(bytes / 4));
+  GPSM_LAUNCHED();
 }
 
 void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint32_t end, uint32_t* bm) {

@@ -52,6 +52,9 @@ struct RefineStamp {
   uint32_t seq = 0;           // this launch
 };
 
+// Copies `bytes` (a multiple of 4) of device memory into ws.h_small at h_dst
+// with a kernel on ws.stream (no copy engine); read after a stream sync.
+void small_to_host(Workspace& ws, void* h_dst, const void* d_src, size_t bytes);
 void launch_mark_range(Workspace& ws, const DeviceGraph& g, uint32_t begin, uint32_t end, uint32_t* bm);
 // stamp/u/prev (optional): skip when C(u) has not changed since the
 // compaction that ran when the last refine seq was `prev` (list and count

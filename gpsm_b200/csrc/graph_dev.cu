@@ -322,6 +322,7 @@ Workspace* workspace_create(int device, size_t arena_bytes, uint32_t max_tiles) 
     GPSM_CUDA(cudaMalloc(&ws->d_heavy, ws->heavy_cap * sizeof(uint32_t)));
     GPSM_CUDA(cudaMalloc(&ws->d_heavy_count, sizeof(uint32_t)));
     GPSM_CUDA(cudaMallocHost(&ws->h_small, 4096 * sizeof(unsigned long long)));
+    GPSM_CUDA(cudaHostGetDevicePointer((void**)&ws->h_small_dev, ws->h_small, 0));
     GPSM_CUDA(cudaEventCreate(&ws->ev0));
     GPSM_CUDA(cudaEventCreate(&ws->evm));
     GPSM_CUDA(cudaEventCreate(&ws->eve0));

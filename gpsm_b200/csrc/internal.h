@@ -144,7 +144,11 @@ struct Workspace {
   ScanState scan;
   uint32_t* d_flags = nullptr;      // [64] device flags and small counters
   unsigned long long* d_small = nullptr;  // [64] device scratch for results of scans
-  unsigned long long* h_small = nullptr;  // pinned mirror
+  unsigned long long* h_small = nullptr;  // pinned mirror (4096 words)
+  // h_small as the device addresses it: small results are written there by
+  // a kernel (small_to_host), not copied by a copy engine, so they never wait
+  // behind the large row copies other slots have queued on the engines
+  unsigned long long* h_small_dev = nullptr;
   cudaEvent_t ev0 = nullptr, evm = nullptr, ev1 = nullptr;
   cudaEvent_t eve0 = nullptr, eve1 = nullptr;  // around each join launch
   cudaEvent_t evb0 = nullptr, evb1 = nullptr;  // around a batch

@@ -41,7 +41,8 @@ def init(device=0, arena_bytes=0, tuning_file=TUNING_FILE):
 
 def set_tuning(**kw):
     """Process-wide launch choices: heavy_degree, ext_blocks_per_sm,
-    step_cands, level_bytes, slots, race_share (unset or 0 = unchanged)."""
+    step_cands, level_bytes, slots, race_share, scan_spin_limit, ext_items,
+    filter_team, explore_team (unset or 0 = unchanged)."""
     lib = _lib.load()
     t = _lib.Tuning()
     for k, v in kw.items():

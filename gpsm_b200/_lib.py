@@ -115,7 +115,7 @@ class MatchInfo(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("heavy_degree", u32), ("ext_blocks_per_sm", u32), ("step_cands", u64), ("level_bytes", u64),
                 ("slots", u32), ("scan_spin_limit", u32), ("race_share", u64),
-                ("ext_items", u32), ("filter_team", u32)]
+                ("ext_items", u32), ("filter_team", u32), ("explore_team", u32), ("pad", u32)]
 
 
 class RequestInfo(C.Structure):

@@ -13,6 +13,7 @@ after a warm-up) under every combination of:
                      its tile is 256 x ext_items candidates; a thread keeps
                      one row's state and list positions across its items)
   filter_team        lanes per candidate in the refinement steps (4, 8 or 32)
+  explore_team       lanes per candidate in the exploration steps (8 or 32)
   step_cands         candidates one join step may admit
   slots              engine slots running queries at once
 and writes the fastest combination to --out; gpsm_b200.init() applies it.
@@ -21,7 +22,8 @@ step budget (a budget whose scratch outgrows L2 slows every long query) and
 a sample of quick queries alone picked the wrong one. --queries N instead
 times N quick queries (device time under --max-ms each).
 The grid keeps what earlier sweeps left open (a 4,096 hub threshold, 6
-check blocks per SM and 4 candidates per check thread won every sweep).
+check blocks per SM, 4 candidates per check thread and the 2^23 step budget
+won every sweep; 32-lane refinement teams lost each time).
 Slot counts are compared one process each (--slots; a process sizes every
 slot pool from the memory left free when the pool is created, so a second
 pool in the same process would get less): the grid keeps one count.
@@ -38,8 +40,8 @@ from . import DeviceGraph, get_tuning, init, match, match_batch, set_tuning
 from . import learned as L
 from . import workloads as W
 
-GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4], filter_team=[4, 8, 32],
-            step_cands=[1 << 23, 1 << 24], slots=[8])
+GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4], filter_team=[4, 8],
+            explore_team=[8, 32], step_cands=[1 << 23], slots=[8])
 NSLICES = 20  # the bench's slices of the batch
 
 

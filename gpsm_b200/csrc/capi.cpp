@@ -355,7 +355,8 @@ int gpsm_set_tuning(const gpsm_tuning* t) {
   if (t->race_share) T.race_share = t->race_share;
   if (t->scan_spin_limit) T.scan_spin_limit = t->scan_spin_limit;
   if (t->ext_items) T.ext_items = t->ext_items >= 8 ? 8u : 4u;
-  if (t->filter_team) T.filter_team = t->filter_team >= 32 ? 32u : 8u;
+  if (t->filter_team) T.filter_team = t->filter_team >= 32 ? 32u : t->filter_team <= 4 ? 4u : 8u;
+  if (t->explore_team) T.explore_team = t->explore_team >= 32 ? 32u : 8u;
   return GPSM_OK;
 }
 
@@ -371,6 +372,8 @@ int gpsm_get_tuning(gpsm_tuning* t) {
   t->race_share = T.race_share;
   t->ext_items = T.ext_items;
   t->filter_team = T.filter_team;
+  t->explore_team = T.explore_team;
+  t->pad = 0;
   return GPSM_OK;
 }
 

@@ -418,10 +418,8 @@ __device__ __forceinline__ uint32_t refine_targets(const RefineStamp& rs, uint32
 // lab_vtx, the vertices of u's label with more than hub_degree neighbours.
 // TEAM: lanes per candidate in the light part (4 or 8: eight or four
 // candidates' chains of loads in flight per warp; 32: one candidate, all
-// lanes over its neighbours). Exploration, which scans every neighbour of
-// the target's label, runs with 32; refinement, which stops at the first
-// neighbour in the target's set, with the tuned size (8 measured 15% faster
-// than 32 on the bench batch, and exploration 16% slower with 8).
+// lanes over its neighbours), a tuning choice for exploration (8 or 32) and
+// refinement (4, 8 or 32) each.
 template <bool EXPLORE, uint32_t TEAM>
 __global__ void __launch_bounds__(256, 4) k_filter_step(GraphView g, const uint32_t* __restrict__ lab_vtx,
                                                      uint32_t hub_begin, uint32_t hub_end, uint32_t hub_degree,
@@ -838,8 +836,11 @@ static void launch_filter_step(Workspace& ws, const DeviceGraph& g, uint32_t u, 
   const size_t smem = (EXPLORE ? 3 : 2) * ntgt * sizeof(uint32_t);
   // exploration scans every neighbour of the target's label: whole warps;
   // refinement stops at the first hit: the tuned team size
-  const uint32_t team = tuning().filter_team;
-  if (EXPLORE || team >= 32)
+  const uint32_t team = EXPLORE ? tuning().explore_team : tuning().filter_team;
+  if (EXPLORE && team < 32)
+    k_filter_step<true, 8><<<light + hubs, 256, smem, ws.stream>>>(
+        view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
+  else if (EXPLORE || team >= 32)
     k_filter_step<EXPLORE, 32><<<light + hubs, 256, smem, ws.stream>>>(
         view(g), g.lab_vtx, hb, he, hub, light, chunk_words(g.words), u, tgt, ntgt, bm, g.words, ws.d_flags, rs);
   else if (team <= 4)

@@ -115,8 +115,10 @@ struct Tuning {
   // candidates per thread of the join check kernel (4 or 8): its tile is
   // 256 x ext_items candidates
   uint32_t ext_items = 4;
-  // lanes per candidate in the refinement steps (8 or 32)
+  // lanes per candidate in the refinement steps (4, 8 or 32)
   uint32_t filter_team = 8;
+  // lanes per candidate in the exploration steps (8 or 32)
+  uint32_t explore_team = 32;
 };
 Tuning& tuning();
 int sm_count();

@@ -315,6 +315,8 @@ typedef struct gpsm_tuning {
                                   and the plain order take turns (default 2^28) */
   uint32_t ext_items;          /* candidates per thread of the join check kernel: 4 or 8 (default 4) */
   uint32_t filter_team;        /* lanes per candidate in the refinement steps: 4, 8 or 32 (default 8) */
+  uint32_t explore_team;       /* lanes per candidate in the exploration steps: 8 or 32 (default 32) */
+  uint32_t pad;
 } gpsm_tuning;
 int gpsm_set_tuning(const gpsm_tuning* t);
 int gpsm_get_tuning(gpsm_tuning* t);

@@ -355,10 +355,13 @@ def run_ours(args):
     free_b, _ = torch.cuda.mem_get_info(local)
     e2e_err, srv = None, None
     d2h, e2e_rows = 0, 0
+    # the leg is bound by the rows' copy to the host: at most 8 server slots,
+    # each with room for the largest queries' joins next to its result buffers
+    e2e_slots = min(slots, 8)
     try:
-        srv = G.Server(dg, slots=slots, cap=cap, order=args.order if args.order == "learned" else None,
+        srv = G.Server(dg, slots=e2e_slots, cap=cap, order=args.order if args.order == "learned" else None,
                        model=model, collect_rows=True, work_cap=work_cap,
-                       slot_arena=min(12 << 30, int(0.8 * free_b / slots)) >> 21 << 21, largest_first=True)
+                       slot_arena=min(12 << 30, int(0.8 * free_b / e2e_slots)) >> 21 << 21, largest_first=True)
         for q in e2e_qs:  # untimed: grows the pool of page-locked result blocks
             srv.submit(q)
         for _ in e2e_qs:
@@ -467,7 +470,7 @@ def run_ours(args):
                      "d2h_gb_per_s": e2e_d2h / 1e9 / e2e_wall,
                      "basis": "request server, slice 0 submitted at once (host query arrays in, every embedding "
                               "row to host memory, largest request first, results taken as they finish), after "
-                              "one untimed pass",
+                              "one untimed pass", "server_slots": e2e_slots,
                      "host_pool": {"blocks": pool1["blocks"], "pinned_gb": pool1["pinned_bytes"] / 1e9,
                                    "grown_in_timed_pass": pool1["grown"] - pool0["grown"],
                                    "grow_ms_in_timed_pass": pool1["grow_ms"] - pool0["grow_ms"]}}),

@@ -12,7 +12,11 @@
 // pool grew). The caller gets the block itself, and gpsm_free gives it back
 // to the pool, so the next request reuses it. The pool pins at most
 // GPSM_HOST_POOL_GB GiB (default: a quarter of the host's memory, at most
-// 64 GiB); past that, queries use the other path. A serving loop needs
+// 64 GiB); at that limit a request takes any free block large enough, or
+// the free blocks (all too small for it) are released to make room; only
+// when blocks in use hold the whole limit do queries use the other path.
+// Result sizes vary from a few hundred MB to a few GB, so without that the
+// pool filled with blocks of the wrong sizes. A serving loop needs
 // blocks for every finished request its client has not collected yet:
 // requests finish out of order, so that can be many more than the slots.
 //
@@ -30,6 +34,7 @@
 #include <map>
 #include <mutex>
 #include <unordered_map>
+#include <vector>
 
 #include "engine.h"
 
@@ -44,6 +49,7 @@ struct HostPool {
   uint64_t pinned = 0;
   uint64_t limit = 0;
   uint64_t grown = 0;     // blocks added since the process started
+  uint64_t evicted = 0;   // free blocks released to make room for larger ones
   double grow_ms = 0;     // host time spent touching and pinning them
   // blocks from cudaHostAlloc instead of malloc'd memory registered with
   // cudaHostRegister (GPSM_HOST_POOL_ALLOC=hostalloc)
@@ -65,14 +71,31 @@ HostPool& pool() {
   return *p;
 }
 
-// A pinned block of at least `bytes`, or null when the pool is at its limit
-// or pinning fails (the caller then uses malloc'd memory). A new block is
-// touched and pinned outside the pool's lock (its size is reserved against
-// the limit first), so other slots keep taking and returning blocks.
+// Unpins and frees a block taken out of the pool (no lock held).
+void pool_release_memory(HostPool& P, void* b) {
+  if (P.host_alloc) {
+    cudaFreeHost(b);
+  } else {
+    cudaHostUnregister(b);
+    free(b);
+  }
+  cudaGetLastError();
+}
+
+// A pinned block of at least `bytes`, or null when pinning fails (the caller
+// then uses malloc'd memory). In order: a free block of about the right size
+// (at most twice it), a new block while the pool is under its limit, any
+// free block large enough, and at the limit with none large enough a new
+// block after the free ones (all too small for this request) are released.
+// A new block is touched and pinned outside the pool's lock (its size is
+// reserved against the limit first), so other slots keep taking and
+// returning blocks.
 void* pool_acquire(uint64_t bytes, uint64_t* cap) {
   HostPool& P = pool();
   // size classes: multiples of 64 MiB
   const uint64_t size = (bytes + (64ull << 20) - 1) & ~((64ull << 20) - 1);
+  std::vector<void*> evicted;
+  bool room = false;
   {
     std::lock_guard<std::mutex> lk(P.mu);
     auto it = P.free_blocks.lower_bound(bytes);
@@ -82,9 +105,27 @@ void* pool_acquire(uint64_t bytes, uint64_t* cap) {
       P.free_blocks.erase(it);
       return b;
     }
-    if (P.pinned + size > P.limit) return nullptr;
-    P.pinned += size;
+    if (P.pinned + size <= P.limit) {
+      room = true;
+    } else if (it != P.free_blocks.end()) {
+      void* b = it->second;  // larger than wanted, but pinned already
+      *cap = it->first;
+      P.free_blocks.erase(it);
+      return b;
+    } else {
+      for (auto e = P.free_blocks.begin(); e != P.free_blocks.end() && P.pinned + size > P.limit;) {
+        evicted.push_back(e->second);
+        P.pinned -= e->first;
+        P.owned.erase(e->second);
+        ++P.evicted;
+        e = P.free_blocks.erase(e);
+      }
+      room = P.pinned + size <= P.limit;
+    }
+    if (room) P.pinned += size;
   }
+  for (void* b : evicted) pool_release_memory(P, b);
+  if (!room) return nullptr;
   const auto t0 = std::chrono::steady_clock::now();
   void* b = nullptr;
   bool ok;

@@ -475,17 +475,22 @@ __global__ void __launch_bounds__(kWriteBlock, 4) k_extend_write(const uint32_t*
       __syncthreads();
       if (gathers) {
         uint32_t* sw = sb + lead + threadIdx.x;  // word (trow, tcol) of the chunk; a group is group*w words
-        for (uint32_t r0 = trow; r0 < nq; r0 += kU * group, sw += kU * group * out_cols) {
+        const uint32_t gw = group * out_cols;     // words per group
+        uint32_t r0 = trow;
+        // whole rounds of kU rows (every row exists: no checks), then the rest
+        for (; r0 + (kU - 1) * group < nq; r0 += kU * group, sw += kU * gw) {
           uint32_t val[kU];
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
-            const uint32_t r = r0 + u * group;
-            const uint2 e = r < nq ? s_kept[r] : make_uint2(0u, 0u);
-            val[u] = (r < nq && !new_col) ? __ldg(inb + (size_t)e.x * cols) : e.y;
+            const uint2 e = s_kept[r0 + u * group];
+            val[u] = new_col ? e.y : __ldg(inb + (size_t)e.x * cols);
           }
 #pragma unroll
-          for (int u = 0; u < kU; ++u)
-            if (r0 + u * group < nq) sw[u * group * out_cols] = val[u];
+          for (int u = 0; u < kU; ++u) sw[u * gw] = val[u];
+        }
+        for (; r0 < nq; r0 += group, sw += gw) {
+          const uint2 e = s_kept[r0];
+          *sw = new_col ? e.y : __ldg(inb + (size_t)e.x * cols);
         }
       }
       proxy_fence_shared();

@@ -82,6 +82,34 @@ __device__ __forceinline__ uint32_t gallop_u32(const uint32_t* __restrict__ a, u
   return lower_bound_u32(a, lo, min(probe, hi), key);
 }
 
+// lower_bound over a whole list a[0, len) whose values spread about evenly
+// over their range (vertex ids are permuted at random when a graph is
+// generated): up to three probes where the key would sit if the values
+// between the known bounds were evenly spread, then a binary search in the
+// gap left. The answer is the exact lower bound whatever the values.
+__device__ __forceinline__ uint32_t search_interp_u32(const uint32_t* __restrict__ a, uint32_t len, uint32_t key) {
+  if (len <= 16) return lower_bound_u32(a, 0, len, key);
+  uint32_t L = 0, H = len - 1;  // a[L] < key <= a[H] once the ends are checked
+  uint32_t vL = __ldg(a), vH = __ldg(a + H);
+  if (key <= vL) return 0;
+  if (key > vH) return len;
+#pragma unroll 1
+  for (int it = 0; it < 3 && H - L > 8; ++it) {
+    const float f = (float)(key - vL) / (float)(vH - vL);  // in (0, 1]
+    uint32_t p = L + 1 + (uint32_t)(f * (float)(H - L - 1));
+    p = min(max(p, L + 1), H - 1);
+    const uint32_t v = __ldg(a + p);
+    if (v < key) {
+      L = p;
+      vL = v;
+    } else {
+      H = p;
+      vH = v;
+    }
+  }
+  return lower_bound_u32(a, L + 1, H, key);  // H when nothing in (L, H) is >= key: a[H] >= key
+}
+
 // Candidate-edge list of data vertex mu (a candidate of w) towards v.
 __device__ __forceinline__ bool locate_list(const BackNbr& b, uint32_t mu, unsigned long long nbrs_total,
                                             unsigned long long* lo, unsigned long long* hi) {
@@ -223,7 +251,7 @@ __device__ __forceinline__ unsigned long long row_of(const unsigned long long* _
 // The tile's kept candidates go to kept[tile * tile_size ...] in candidate
 // order, their number to tile_cnt[tile].
 template <int ITEMS>
-__global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
+__global__ void __launch_bounds__(kExtBlock, ITEMS == 4 ? 5 : 3) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
                                                            unsigned long long row_begin,
                                                            const BackNbr* __restrict__ back, uint32_t nb,
                                                            const uint4* __restrict__ drv,
@@ -349,7 +377,7 @@ __global__ void __launch_bounds__(kExtBlock) k_extend_check(const uint32_t* __re
             const uint4 g2 = __ldg(rng + (unsigned long long)cur * nb + j);
             list = S.back[j].nbrs + (((unsigned long long)g2.y << 32) | g2.x);
             len = g2.z;
-            pos = lower_bound_u32(list, 0, len, ky[k]);
+            pos = search_interp_u32(list, len, ky[k]);
           } else {
             pos = gallop_u32(list, pos, len, ky[k]);
           }

@@ -281,7 +281,10 @@ struct Level {
   uint64_t cap_rows = 0;
   uint64_t nrows = 0;
   uint64_t next = 0;
-  double ratio = 4.0;  // observed outputs per input row of the last launch
+  double ratio = 4.0;  // observed candidates per input row of the last step from this level
+  // share of candidates the last step from this level kept, with headroom
+  // (1: a step admits no more candidates than its output holds rows)
+  double keep = 1.0;
 };
 
 }  // namespace
@@ -749,6 +752,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   StepState* d_st2 = arena_alloc<StepState>(ws, 2);
   uint32_t st_turn = 0;
   StepState* h_st = reinterpret_cast<StepState*>(ws.h_small + 1024);
+  StepState* h_st_dev = reinterpret_cast<StepState*>(ws.h_small_dev + 1024);  // h_st as the device writes it
   JoinScratch js;
   uint32_t max_nb = 1;
   for (uint32_t p = 1; p < qn; ++p) max_nb = std::max(max_nb, back_cnt[p]);
@@ -896,6 +900,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     emitted = n1;
     R.stats.level_rows[1] = n1;
   }
+  bool safe_step = false;  // the next step admits no more candidates than its output holds rows
   while (qn > 1 && !capped) {
     // deepest level with rows left
     int lv = -1;
@@ -910,6 +915,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     uint32_t* out;
     uint64_t out_cap, budget;
     bool partial = false;
+    bool cut_rows = false;
     if (final_level && opt.directed) {
       uint64_t space = res_cap - res_used;
       if (space == 0) {
@@ -959,7 +965,13 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
         return GPSM_ERR_BUDGET;
       }
       B.cap_rows = out_cap;
-      budget = std::min<uint64_t>(out_cap, opt.step_cands);
+      // a level that keeps few of its candidates (dense steps: other placed
+      // neighbours' lists reject most) may admit up to out_cap / keep of
+      // them; if more rows are kept than out_cap after all, the write pass
+      // ends the step at a row boundary and the rest are offered again
+      budget = std::min<uint64_t>(opt.step_cands, safe_step ? out_cap : (uint64_t)((double)out_cap / A.keep));
+      budget = std::max<uint64_t>(budget, std::min<uint64_t>(out_cap, opt.step_cands));
+      cut_rows = budget > out_cap;
     }
     // rows offered to this step: enough to fill the budget at the observed
     // candidates per row, within the per-row scratch
@@ -969,20 +981,23 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     StepState* d_st = d_st2 + st_turn;
     StepState* d_next = d_st2 + (st_turn ^ 1);
     st_turn ^= 1;
+    *h_st = StepState{};  // the stream is idle: the step's write pass refills it
     GPSM_CUDA(cudaEventRecord(ws.eve0, s));
     launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                     out_cap, js, d_st, d_next, d_inj + inj_off[lv], inj_cnt[lv]);
+                     out_cap, js, d_st, d_next, d_inj + inj_off[lv], inj_cnt[lv], cut_rows, h_st_dev);
+    safe_step = false;
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 4;  // locate, check, scan, write
     ++R.stats.join_steps;
-    small_to_host(ws, h_st, d_st, sizeof(StepState));
-    GPSM_CUDA(cudaStreamSynchronize(s));
+    GPSM_CUDA(cudaStreamSynchronize(s));  // the write pass filled h_st
     {
       float ems = 0;
       GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
       R.stats.expand_ms += ems;
     }
     const uint64_t admitted = h_st->rows, written = h_st->written, cands = h_st->cands;
+    const bool was_cut = h_st->cut != 0;
+    const uint64_t cands_done = was_cut ? h_st->cands_done : cands;  // candidates of the rows written whole
     if (trace_enabled()) {
       float ems = 0;
       cudaEventElapsedTime(&ems, ws.eve0, ws.eve1);
@@ -990,9 +1005,24 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
                                     written * 4ull * (lv + 1);
       fprintf(stderr,
               "[gpsm] step level=%d nb=%u rows=[%llu,%llu) admitted=%llu cands=%llu written=%llu budget=%llu "
-              "alg_bytes=%llu ms=%.3f\n",
+              "alg_bytes=%llu ms=%.3f%s\n",
               lv, back_cnt[lv], (unsigned long long)rb, (unsigned long long)re, (unsigned long long)admitted,
-              (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ab, ems);
+              (unsigned long long)cands, (unsigned long long)written, (unsigned long long)budget, ab, ems,
+              was_cut ? " cut" : "");
+    }
+    if (was_cut && admitted == 0) {
+      // the first row alone keeps more than the output holds at this budget:
+      // offer it again with no more candidates than rows fit (the checked
+      // candidates still count as work)
+      cands_total += cands;
+      R.stats.cands_scanned += cands;
+      A.keep = 1.0;
+      safe_step = true;
+      if (limit && cands_total >= limit) {
+        hit_limit = true;
+        break;
+      }
+      continue;
     }
     if (admitted == 0) {
       if (final_level && !partial && res_used > 0) {  // make room and retry
@@ -1006,7 +1036,9 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
       set_last_error("a single row has more candidates than a join step admits");
       return GPSM_ERR_BUDGET;
     }
-    A.ratio = std::max(1.0 / 1024.0, (double)cands / (double)admitted);
+    A.ratio = std::max(1.0 / 1024.0, (double)cands_done / (double)admitted);
+    if (!final_level && cands_done > 0)  // kept share with 1.5x headroom, at least 1/64
+      A.keep = std::min(1.0, std::max(1.0 / 64.0, 1.5 * (double)written / (double)cands_done));
     A.next = rb + admitted;
     alg_bytes += admitted * 4ull * lv + admitted * 24ull * back_cnt[lv] + cands * 4ull + written * 4ull * (lv + 1);
     uint64_t kept = written;

@@ -105,6 +105,11 @@ struct StepState {
   unsigned long long verified;     // directed mode: rows that passed the verify filter (host copy)
   unsigned long long cand_end;     // end offset of the last admitted row's candidates
   unsigned long long full;         // a row failed admission: later locate tiles skip their rows
+  // the write pass cut the output at a row boundary (more kept rows than
+  // out_cap): rows and written were reduced to the rows written whole,
+  // cands_done is their candidates (cands stays all that were checked)
+  unsigned long long cut;
+  unsigned long long cands_done;
 };
 
 // Per-row scratch of a join step: driver list (lo, hi32 of lo, length, j)
@@ -136,10 +141,14 @@ uint64_t join_kept_slack();
 // neighbours are back[0..nb) into `out` (in_cols+1 columns), at most out_cap
 // rows (the first out_cap in order). nbrs_total bounds every list range.
 // d_inj[0..ninj): the input columns whose query vertex has the new vertex's
-// label (the only columns a candidate can repeat).
+// label (the only columns a candidate can repeat). cut_rows: when more rows
+// are kept than out_cap, the step ends at a row boundary instead (rows and
+// written count only the rows written whole; the rest are offered again).
+// host_st: the device address of a page-locked StepState the write pass
+// fills with the step's final state.
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
-                      const uint32_t* d_inj, uint32_t ninj);
+                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st);
 
 }  // namespace gpsm

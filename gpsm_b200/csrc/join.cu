@@ -465,8 +465,10 @@ __global__ void __launch_bounds__(kWriteBlock, 4) k_extend_write(const uint32_t*
                                                                  uint32_t ntiles_max, uint32_t ext_tile,
                                                                  uint32_t* __restrict__ out,
                                                                  unsigned long long out_cap,
-                                                                 StepState* __restrict__ st,
-                                                                 StepState* __restrict__ next) {
+                                                                 const unsigned long long* __restrict__ coff,
+                                                                 uint32_t cut_rows, StepState* __restrict__ st,
+                                                                 StepState* __restrict__ next,
+                                                                 StepState* __restrict__ host_st) {
   constexpr int kU = 4;
   __shared__ __align__(128) uint32_t sbuf[2][kWriteStage + 4];
   __shared__ uint2 s_kept[kWriteRows];
@@ -479,7 +481,42 @@ __global__ void __launch_bounds__(kWriteBlock, 4) k_extend_write(const uint32_t*
   const bool new_col = tcol == cols;  // this thread writes the new value
   const uint32_t* __restrict__ inb = in + row_begin * cols + tcol;  // column tcol of row r: inb + r * cols
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->written = min(tile_off[ntiles_max], out_cap);
+    const unsigned long long total = tile_off[ntiles_max];
+    if (cut_rows && total > out_cap) {
+      // more kept rows than the output holds: keep only the input rows whose
+      // outputs all fit. Outputs are in input-row order, so if r is the row
+      // of output out_cap, the rows before r are whole and start no later
+      // than r's first output. Output p is entry p - tile_off[T] of tile T.
+      uint32_t lo = 0, hi = ntiles_max;  // tile_off[lo] <= out_cap < tile_off[hi]
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tile_off[mid] <= out_cap) lo = mid;
+        else hi = mid;
+      }
+      const uint32_t r = kept[(unsigned long long)lo * ext_tile + (out_cap - tile_off[lo])].x;
+      // row r's first candidate lies in tile t0; that tile's kept rows before
+      // r are the last outputs of the whole rows
+      const unsigned long long cr = coff[r];
+      const uint32_t t0 = (uint32_t)(cr / ext_tile);
+      const uint2* k0 = kept + (unsigned long long)t0 * ext_tile;
+      uint32_t a = 0, b = (uint32_t)(tile_off[t0 + 1] - tile_off[t0]);  // entries of tile t0
+      while (a < b) {
+        const uint32_t m = (a + b) >> 1;
+        if (k0[m].x < r) a = m + 1;
+        else b = m;
+      }
+      st->written = tile_off[t0] + a;
+      st->rows = r;
+      st->cands_done = cr;
+      st->cut = 1;
+    } else {
+      st->written = min(total, out_cap);
+      st->cands_done = st->cands;
+    }
+    // the step's final state, straight into the host's page-locked mirror
+    // (read after the stream is synchronised)
+    *host_st = *st;
+    __threadfence_system();
     *next = StepState{};  // the next step starts from zero
   }
   uint32_t chunk_no = 0;  // chunks this block has issued (selects the staging buffer)
@@ -601,7 +638,7 @@ uint64_t join_kept_slack() { return 2ull * kMaxExtTile; }
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
-                      const uint32_t* d_inj, uint32_t ninj) {
+                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
   const uint32_t items = ext_items();
@@ -642,7 +679,7 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));
   k_extend_write<<<wgrid, kWriteBlock, 0, ws.stream>>>(in, in_cols, row_begin, js.kept, js.tile_cnt, js.tile_off,
                                                (uint32_t)std::max<uint64_t>(ntiles_max, 1), ext_tile, out, out_cap,
-                                               d_st, d_next);
+                                               js.coff, cut_rows ? 1u : 0u, d_st, d_next, host_st);
   GPSM_LAUNCHED();
 }
 

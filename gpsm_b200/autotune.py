@@ -41,7 +41,7 @@ from . import learned as L
 from . import workloads as W
 
 GRID = dict(heavy_degree=[4096], ext_blocks_per_sm=[6], ext_items=[4], filter_team=[4, 8],
-            explore_team=[8, 32], step_cands=[1 << 23], slots=[8])
+            explore_team=[8, 32], step_cands=[1 << 23], slots=[12])
 NSLICES = 20  # the bench's slices of the batch
 
 
@@ -54,6 +54,7 @@ def main():
     ap.add_argument("--cap", type=int, default=10_000_000)
     ap.add_argument("--max-ms", type=float, default=200.0)
     ap.add_argument("--slots", type=int, default=0, help="the slot count to tune at (0 = the grid's)")
+    ap.add_argument("--grid", default="", help='JSON object replacing grid entries, e.g. {"step_cands": [8388608]}')
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
                                                   "tuning.json"))
     args = ap.parse_args()
@@ -75,6 +76,11 @@ def main():
         nq = len(wl.queries)
         for sl in (int(x) for x in args.slices.split(",")):
             sample.extend(wl.queries[nq * sl // NSLICES: nq * (sl + 1) // NSLICES])
+    if args.grid:
+        for k, v in json.loads(args.grid).items():
+            if k not in GRID:
+                raise SystemExit(f"unknown grid entry {k}")
+            GRID[k] = list(v)
     if args.slots:
         GRID["slots"] = [args.slots]
     results = []

@@ -109,7 +109,7 @@ class MatchInfo(C.Structure):
                 ("expand_launches", u64), ("filter_launches", u64), ("alg_bytes_join", u64),
                 ("expand_ms", f64), ("plan_ms", f64), ("predicted_work", f64), ("predicted_peak", f64),
                 ("order_fallback", i32), ("aborted", i32), ("predicted_work_plain", f64),
-                ("order_attempts", u32), ("pad2", u32), ("cands_scanned", u64)]
+                ("order_attempts", u32), ("pad2", u32), ("cands_scanned", u64), ("cut_steps", u64)]
 
 
 class Tuning(C.Structure):

@@ -111,6 +111,7 @@ void fill_info(const MatchResult& R, gpsm_match_info* info) {
   info->predicted_work_plain = R.stats.predicted_work_plain;
   info->order_attempts = R.stats.order_attempts;
   info->cands_scanned = R.stats.cands_scanned;
+  info->cut_steps = R.stats.cut_steps;
 }
 
 }  // namespace

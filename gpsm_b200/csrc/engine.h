@@ -98,6 +98,7 @@ struct MatchStats {
   std::vector<uint64_t> level_cands;     // candidates scanned when extending width w
   uint64_t expand_launches = 0;
   uint64_t join_steps = 0;      // join steps (each: locate, check, scan, write)
+  uint64_t cut_steps = 0;       // steps the write pass ended at a row boundary
   uint64_t filter_launches = 0;
   double device_ms = 0;
   double filter_ms = 0, join_ms = 0;

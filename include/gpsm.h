@@ -170,6 +170,8 @@ typedef struct gpsm_match_info {
   uint32_t order_attempts;   /* learned order: join attempts of the two orders (0: no race) */
   uint32_t pad2;
   uint64_t cands_scanned;    /* candidates the joins scanned, over all attempts */
+  uint64_t cut_steps;        /* join steps that kept more rows than their output held and ended
+                                at a row boundary (the rest offered again) */
 } gpsm_match_info;
 
 typedef struct gpsm_batch_info {

@@ -1,0 +1,30 @@
+"""Join steps that end at a row boundary: with GPSM_DEBUG_WIDE_STEPS=1 every
+intermediate step admits 64 times the candidates its output holds rows, so
+nearly every step keeps more rows than fit and the write pass ends it at a
+row boundary (the rest offered again). The rows must be exactly those of
+the default steps."""
+import os
+
+import numpy as np
+import pytest
+
+from gpsm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def test_steps_cut_at_a_row_boundary_give_the_same_rows(gpu):
+    wl = W.workload("rmat20_mix", count=8)
+    dg = gpu.DeviceGraph(wl.graph)
+    # small levels: many steps per query, so many of them are cut
+    ref = [gpu.match(dg, q, cap=100_000, level_bytes=8 << 20) for q in wl.queries]
+    os.environ["GPSM_DEBUG_WIDE_STEPS"] = "1"
+    try:
+        wide = [gpu.match(dg, q, cap=100_000, level_bytes=8 << 20) for q in wl.queries]
+    finally:
+        del os.environ["GPSM_DEBUG_WIDE_STEPS"]
+    assert sum(o.info["cut_steps"] for o in wide) > 0
+    for r, o in zip(ref, wide):
+        assert o.count == r.count
+        assert np.array_equal(o.pos2id, r.pos2id)
+        assert np.array_equal(o.rows, r.rows)

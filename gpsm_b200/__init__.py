@@ -94,6 +94,14 @@ class DeviceGraph:
         _lib.check(self._lib.gpsm_graph_download(self.handle, _lib.ptr(off), _lib.ptr(cols)), "gpsm_graph_download")
         return off, cols[: nnz.value]
 
+    def edge_table(self):
+        """(slots, longest probe) of the edge table built at upload; slots
+        0 when it was not built (the joins then search the lists)."""
+        slots, probe = C.c_uint64(), C.c_uint32()
+        _lib.check(self._lib.gpsm_graph_edge_table(self.handle, C.byref(slots), C.byref(probe)),
+                   "gpsm_graph_edge_table")
+        return slots.value, probe.value
+
     def set_directed(self, edges, labels=None):
         """Directed, labelled data edges (pairs (from, to) as in the file)
         for directed matching (IO::verify's test on the device)."""

@@ -58,6 +58,7 @@ SIGNATURES = {
     "gpsm_graph_upload": (C.c_int, [vp, vp, vp, u32, vp]),
     "gpsm_graph_free": (C.c_int, [vp]),
     "gpsm_graph_info": (C.c_int, [vp, vp, vp, vp]),
+    "gpsm_graph_edge_table": (C.c_int, [vp, vp, vp]),
     "gpsm_graph_set_directed": (C.c_int, [vp, u64, vp, vp]),
     "gpsm_graph_build": (C.c_int, [vp, u64, vp, u32, vp]),
     "gpsm_graph_download": (C.c_int, [vp, vp, vp]),

@@ -250,6 +250,13 @@ int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_de
   return GPSM_OK;
 }
 
+int gpsm_graph_edge_table(gpsm_graph_t g, uint64_t* slots, uint32_t* max_probe) {
+  if (!g) return GPSM_ERR_INVALID;
+  if (slots) *slots = g->g->ehash ? (1ull << g->g->ehash_bits) : 0;
+  if (max_probe) *max_probe = g->g->ehash ? g->g->ehash_probe : 0;
+  return GPSM_OK;
+}
+
 int gpsm_engine_match(gpsm_engine_t eng, gpsm_graph_t g, uint32_t qn, const uint32_t* q_labels, uint32_t qm,
                       const uint32_t* q_edges, const gpsm_match_opts* opts, uint32_t** out_rows, int32_t* id_map,
                       int32_t* pos2id, gpsm_match_info* info) {

@@ -242,6 +242,81 @@ __global__ void k_label_runs_write(const uint32_t* __restrict__ off, const unsig
   }
 }
 
+// A warp per vertex u inserts its edges (u, b) with u < b: a slot holds the
+// key or, if empty, takes it by compare-and-swap; otherwise the next slot.
+// The longest distance from a key's home slot goes to *probe; a key that
+// would go farther than kMaxProbe sets DF_OVERFLOW and is dropped (the
+// table is then not used).
+constexpr uint32_t kMaxProbe = 4096;
+
+__global__ void k_edge_hash_build(const uint32_t* __restrict__ off, const uint32_t* __restrict__ col, uint32_t n,
+                                  unsigned long long* __restrict__ table, uint32_t bits, uint32_t* __restrict__ probe,
+                                  uint32_t* __restrict__ flags) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const unsigned long long mask = (1ull << bits) - 1;
+  uint32_t longest = 0;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += nwarps) {
+    const uint32_t e = off[u + 1];
+    for (uint32_t j = off[u] + lane; j < e; j += 32) {
+      const uint32_t b = col[j];
+      if (b <= u) continue;
+      const unsigned long long key = (unsigned long long)u << 32 | b;
+      unsigned long long s = (key * 0x9E3779B97F4A7C15ull) >> (64 - bits);
+      uint32_t d = 0;
+      for (;; ++d) {
+        if (d > kMaxProbe) {
+          atomicOr(flags, (uint32_t)DF_OVERFLOW);
+          break;
+        }
+        const unsigned long long prev = atomicCAS(table + s, ~0ull, key);
+        if (prev == ~0ull || prev == key) break;
+        s = (s + 1) & mask;
+      }
+      longest = max(longest, d);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+  if (lane == 0 && longest) atomicMax(probe, longest);
+}
+
+void build_edge_hash(DeviceGraph& g) {
+  const uint64_t edges = g.nnz / 2;
+  if (edges == 0) return;
+  uint32_t bits = 10;
+  while ((1ull << bits) < 2 * edges) ++bits;  // at most half full
+  const size_t bytes = (size_t)8 << bits;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || bytes > free_b / 4) {
+    cudaGetLastError();
+    return;  // the joins search the lists instead
+  }
+  unsigned long long* table = nullptr;
+  uint32_t* d_aux = nullptr;  // [0] longest probe, [1] flags
+  if (cudaMalloc(&table, bytes) != cudaSuccess || cudaMalloc(&d_aux, 8) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(table);
+    cudaFree(d_aux);
+    return;
+  }
+  uint32_t aux[2] = {0, 0};
+  bool ok = cudaMemset(table, 0xff, bytes) == cudaSuccess && cudaMemset(d_aux, 0, 8) == cudaSuccess;
+  if (ok) {
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(((uint64_t)g.n * 32 + 255) / 256, 148 * 64);
+    k_edge_hash_build<<<grid, 256>>>(g.off, g.col, g.n, table, bits, d_aux, d_aux + 1);
+    ok = cudaGetLastError() == cudaSuccess && cudaMemcpy(aux, d_aux, 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  cudaFree(d_aux);
+  if (!ok || (aux[1] & DF_OVERFLOW)) {
+    cudaGetLastError();
+    cudaFree(table);
+    return;
+  }
+  g.ehash = table;
+  g.ehash_bits = bits;
+  g.ehash_probe = aux[0];
+}
+
 void build_label_runs(DeviceGraph& g, const uint32_t* h_lab) {
   const uint32_t n = g.n;
   const uint64_t nnz = g.nnz;

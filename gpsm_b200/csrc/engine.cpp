@@ -908,6 +908,12 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     const char* e = getenv("GPSM_DEBUG_WIDE_STEPS");
     return e && e[0] == '1';
   }();
+  // GPSM_DEBUG_NO_EDGE_HASH=1: search the candidate-edge lists even when the
+  // graph has its edge table (the two must give the same rows)
+  const bool use_hash = [] {
+    const char* e = getenv("GPSM_DEBUG_NO_EDGE_HASH");
+    return !(e && e[0] == '1');
+  }();
   while (qn > 1 && !capped) {
     // deepest level with rows left
     int lv = -1;
@@ -992,7 +998,8 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     *h_st = StepState{};  // the stream is idle: the step's write pass refills it
     GPSM_CUDA(cudaEventRecord(ws.eve0, s));
     launch_join_step(ws, A.buf, (uint32_t)lv, rb, re, d_back + back_off[lv], back_cnt[lv], nbrs_total, budget, out,
-                     out_cap, js, d_st, d_next, d_inj + inj_off[lv], inj_cnt[lv], cut_rows, h_st_dev);
+                     out_cap, js, d_st, d_next, d_inj + inj_off[lv], inj_cnt[lv], cut_rows, h_st_dev,
+                     use_hash ? g.ehash : nullptr, g.ehash_bits, g.ehash_probe);
     safe_step = false;
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 4;  // locate, check, scan, write

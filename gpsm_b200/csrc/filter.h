@@ -22,6 +22,26 @@ inline GraphView view(const DeviceGraph& g) {
 // Builds g.lcol / g.run_off / g.runs on the device (leaves them null when
 // vertex ids and label ranks do not fit one 32-bit key).
 void build_label_runs(DeviceGraph& g, const uint32_t* h_lab);
+// Builds g.ehash from the CSR (leaves it null when the table does not fit
+// the free memory or a probe sequence grows past its limit).
+void build_edge_hash(DeviceGraph& g);
+
+#ifdef __CUDACC__
+// Whether data edge (a, b) exists, from g.ehash (a != b).
+__device__ __forceinline__ bool edge_in_hash(const unsigned long long* __restrict__ table, uint32_t bits,
+                                             uint32_t probe, uint32_t a, uint32_t b) {
+  const unsigned long long key = a < b ? ((unsigned long long)a << 32 | b) : ((unsigned long long)b << 32 | a);
+  const unsigned long long mask = (1ull << bits) - 1;
+  unsigned long long s = (key * 0x9E3779B97F4A7C15ull) >> (64 - bits);
+  for (uint32_t p = 0; p <= probe; ++p) {
+    const unsigned long long k = __ldg(table + s);
+    if (k == key) return true;
+    if (k == ~0ull) return false;
+    s = (s + 1) & mask;
+  }
+  return false;
+}
+#endif
 
 // Candidates deferred by a warp kernel to a block-per-candidate kernel.
 struct HeavyList {
@@ -145,10 +165,13 @@ uint64_t join_kept_slack();
 // are kept than out_cap, the step ends at a row boundary instead (rows and
 // written count only the rows written whole; the rest are offered again).
 // host_st: the device address of a page-locked StepState the write pass
-// fills with the step's final state.
+// fills with the step's final state. ehash (null: none): the data graph's
+// edge table (DeviceGraph::ehash), which replaces the list searches of steps
+// with more than one placed neighbour.
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
-                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st);
+                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st,
+                      const unsigned long long* ehash, uint32_t ehash_bits, uint32_t ehash_probe);
 
 }  // namespace gpsm

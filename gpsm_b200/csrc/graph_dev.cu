@@ -121,6 +121,7 @@ static DeviceGraph* graph_finish(int device, uint32_t n, const uint32_t* off, co
     GPSM_LAUNCHED();
     GPSM_CUDA(cudaDeviceSynchronize());
     build_label_runs(*g, lab);
+    build_edge_hash(*g);
   } catch (...) {
     cudaFree(g->off);
     cudaFree(g->col);
@@ -224,6 +225,7 @@ DeviceGraph* graph_upload(int device, const uint32_t* off, const uint32_t* col, 
     GPSM_LAUNCHED();
     GPSM_CUDA(cudaDeviceSynchronize());
     build_label_runs(*g, lab);
+    build_edge_hash(*g);
   } catch (...) {
     cudaFree(g->off);
     cudaFree(g->col);
@@ -293,6 +295,7 @@ void graph_free(DeviceGraph* g) {
   cudaFree(g->lcol);
   cudaFree(g->run_off);
   cudaFree(g->runs);
+  cudaFree(g->ehash);
   delete g;
 }
 

@@ -71,6 +71,14 @@ struct DeviceGraph {
   uint32_t* lcol = nullptr;     // [nnz] or null (not built)
   uint32_t* run_off = nullptr;  // [n+1] directory offsets per vertex
   uint2* runs = nullptr;        // [run_off[n]] (label, index into lcol), labels ascending per vertex
+  // every undirected edge once, as (smaller << 32 | larger), in an open-
+  // addressing table of 2^ehash_bits slots (all ones: empty), at most half
+  // full, probed linearly; no lookup needs more than ehash_probe + 1 slots.
+  // The join checks a candidate against a placed neighbour's list with one
+  // lookup here (null: not built, the list is searched)
+  unsigned long long* ehash = nullptr;
+  uint32_t ehash_bits = 0;
+  uint32_t ehash_probe = 0;
   // label frequency as the reference computes it (Graph::inverse_num)
   uint64_t label_count(uint32_t label) const;
   // [begin, end) of lab_vtx for vertices with `label` and degree >= d

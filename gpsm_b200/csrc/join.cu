@@ -250,8 +250,13 @@ __device__ __forceinline__ unsigned long long row_of(const unsigned long long* _
 //      for the next candidate starts where the previous one ended.
 // The tile's kept candidates go to kept[tile * tile_size ...] in candidate
 // order, their number to tile_cnt[tile].
-template <int ITEMS>
-__global__ void __launch_bounds__(kExtBlock, ITEMS == 4 ? 5 : 3) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
+//
+// HASH: pass 2 asks the data graph's edge table instead: y is in w's list
+// N(row[w]) ∩ C(v) exactly when edge (row[w], y) exists, since y comes from
+// the driver list and so is in C(v) already; one lookup of the same cost
+// for every candidate, where the list search takes as long as its gap.
+template <int ITEMS, bool HASH>
+__global__ void __launch_bounds__(kExtBlock, ITEMS == 4 ? (HASH ? 4 : 5) : 3) k_extend_check(const uint32_t* __restrict__ in, uint32_t cols,
                                                            unsigned long long row_begin,
                                                            const BackNbr* __restrict__ back, uint32_t nb,
                                                            const uint4* __restrict__ drv,
@@ -260,7 +265,9 @@ __global__ void __launch_bounds__(kExtBlock, ITEMS == 4 ? 5 : 3) k_extend_check(
                                                            const uint32_t* __restrict__ tile_row,
                                                            uint2* __restrict__ kept, uint32_t* __restrict__ tile_cnt,
                                                            StepState* __restrict__ st,
-                                                           const uint32_t* __restrict__ inj, uint32_t ninj) {
+                                                           const uint32_t* __restrict__ inj, uint32_t ninj,
+                                                           const unsigned long long* __restrict__ ehash,
+                                                           uint32_t ehash_bits, uint32_t ehash_probe) {
   constexpr uint32_t kTile = kExtBlock * ITEMS;
   __shared__ ExtendShared S;
   stage_back(S.back, back, nb);
@@ -365,7 +372,21 @@ __global__ void __launch_bounds__(kExtBlock, ITEMS == 4 ? 5 : 3) k_extend_check(
         keep |= (ok ? 1u : 0u) << k;
       }
       // pass 2: y must lie in every other placed neighbour's list
-      for (uint32_t j = 0; keep && j < nb; ++j) {
+      if (HASH) {
+        for (uint32_t j = 0; keep && j < nb; ++j) {
+          uint32_t cur = 0xffffffffu, wv = 0;  // this row's value in w's column
+#pragma unroll
+          for (int k = 0; k < ITEMS; ++k) {
+            if (!((keep >> k) & 1u) || kd[k] == j) continue;
+            if (kr[k] != cur) {
+              cur = kr[k];
+              wv = __ldg(in + (row_begin + cur) * cols + S.back[j].col);
+            }
+            if (!edge_in_hash(ehash, ehash_bits, ehash_probe, wv, ky[k])) keep &= ~(1u << k);
+          }
+        }
+      }
+      for (uint32_t j = 0; !HASH && keep && j < nb; ++j) {
         uint32_t cur = 0xffffffffu;
         const uint32_t* __restrict__ list = nullptr;  // this row's list towards v, from its first entry
         uint32_t pos = 0, len = 0;
@@ -584,21 +605,22 @@ __global__ void __launch_bounds__(kWriteBlock, 4) k_extend_write(const uint32_t*
 
 // Blocks of k_extend_check<ITEMS> one SM holds at once (registers and shared
 // memory decide it); asked once per process.
-template <int ITEMS>
+template <int ITEMS, bool HASH>
 static uint32_t ext_resident_per_sm() {
   static const uint32_t n = [] {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend_check<ITEMS>, kExtBlock, 0) != cudaSuccess || b < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend_check<ITEMS, HASH>, kExtBlock, 0) != cudaSuccess ||
+        b < 1)
       b = 1;
     return (uint32_t)b;
   }();
   return n;
 }
 
-template <int ITEMS>
+template <int ITEMS, bool HASH>
 static uint32_t ext_grid() {  // persistent extend blocks: all resident at once
   const uint32_t per_sm =
-      std::min<uint32_t>(std::max<uint32_t>(1, tuning().ext_blocks_per_sm), ext_resident_per_sm<ITEMS>());
+      std::min<uint32_t>(std::max<uint32_t>(1, tuning().ext_blocks_per_sm), ext_resident_per_sm<ITEMS, HASH>());
   return (uint32_t)sm_count() * per_sm;
 }
 
@@ -638,7 +660,8 @@ uint64_t join_kept_slack() { return 2ull * kMaxExtTile; }
 void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint64_t row_begin, uint64_t row_end,
                       const BackNbr* d_back, uint32_t nb, uint64_t nbrs_total, uint64_t budget, uint32_t* out,
                       uint64_t out_cap, const JoinScratch& js, StepState* d_st, StepState* d_next,
-                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st) {
+                      const uint32_t* d_inj, uint32_t ninj, bool cut_rows, StepState* host_st,
+                      const unsigned long long* ehash, uint32_t ehash_bits, uint32_t ehash_probe) {
   const uint64_t nrows = row_end - row_begin;
   if (nrows == 0) return;
   const uint32_t items = ext_items();
@@ -666,14 +689,24 @@ void launch_join_step(Workspace& ws, const uint32_t* in, uint32_t in_cols, uint6
   GPSM_LAUNCHED();
   // check pass: persistent blocks take tiles from a counter until the
   // admitted candidates run out
-  if (items == 8)
-    k_extend_check<8><<<ext_grid<8>(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng,
-                                                                  js.coff, js.tile_row, js.kept, js.tile_cnt, d_st,
-                                                                  d_inj, ninj);
-  else
-    k_extend_check<4><<<ext_grid<4>(), kExtBlock, 0, ws.stream>>>(in, in_cols, row_begin, d_back, nb, js.drv, js.rng,
-                                                                  js.coff, js.tile_row, js.kept, js.tile_cnt, d_st,
-                                                                  d_inj, ninj);
+  if (ehash && nb > 1) {
+    if (items == 8)
+      k_extend_check<8, true><<<ext_grid<8, true>(), kExtBlock, 0, ws.stream>>>(
+          in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff, js.tile_row, js.kept, js.tile_cnt, d_st, d_inj,
+          ninj, ehash, ehash_bits, ehash_probe);
+    else
+      k_extend_check<4, true><<<ext_grid<4, true>(), kExtBlock, 0, ws.stream>>>(
+          in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff, js.tile_row, js.kept, js.tile_cnt, d_st, d_inj,
+          ninj, ehash, ehash_bits, ehash_probe);
+  } else if (items == 8) {
+    k_extend_check<8, false><<<ext_grid<8, false>(), kExtBlock, 0, ws.stream>>>(
+        in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff, js.tile_row, js.kept, js.tile_cnt, d_st, d_inj,
+        ninj, nullptr, 0, 0);
+  } else {
+    k_extend_check<4, false><<<ext_grid<4, false>(), kExtBlock, 0, ws.stream>>>(
+        in, in_cols, row_begin, d_back, nb, js.drv, js.rng, js.coff, js.tile_row, js.kept, js.tile_cnt, d_st, d_inj,
+        ninj, nullptr, 0, 0);
+  }
   GPSM_LAUNCHED();
   launch_scan_u32(ws, js.tile_cnt, std::max<uint64_t>(ntiles_max, 1), js.tile_off);
   const uint32_t wgrid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ntiles_max, (uint64_t)sm_count() * 8));

@@ -109,6 +109,10 @@ int gpsm_graph_build(const uint32_t* edges, uint64_t m, const uint32_t* labels, 
 /* Copies a device graph's CSR back (offsets[n+1], cols[offsets[n]]; either may be NULL). */
 int gpsm_graph_download(gpsm_graph_t g, uint32_t* offsets, uint32_t* cols);
 int gpsm_graph_info(gpsm_graph_t g, uint32_t* n, uint64_t* nnz, uint32_t* max_degree);
+/* The edge table built at upload (no counterpart in the reference): slots
+ * (0: not built, the joins search the candidate-edge lists) and the longest
+ * probe a lookup needs. */
+int gpsm_graph_edge_table(gpsm_graph_t g, uint64_t* slots, uint32_t* max_probe);
 /* Attaches the data graph's directed, edge-labelled edges (m pairs (from, to)
  * as in the file, labels[m] or NULL = 1) for GPSM_F_DIRECTED. The reference
  * keeps them in Graph::vertices[].out (graph/Graph.cpp:20-24). */

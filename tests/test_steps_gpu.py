@@ -28,3 +28,25 @@ def test_steps_cut_at_a_row_boundary_give_the_same_rows(gpu):
         assert o.count == r.count
         assert np.array_equal(o.pos2id, r.pos2id)
         assert np.array_equal(o.rows, r.rows)
+
+
+def test_edge_table_and_list_search_give_the_same_rows(gpu):
+    """Steps with more than one placed neighbour check candidates in the
+    data graph's edge table; GPSM_DEBUG_NO_EDGE_HASH=1 makes them search the
+    candidate-edge lists instead. Dense queries give the same rows either way."""
+    wl = W.workload("rmat20_mix", count=10)
+    dg = gpu.DeviceGraph(wl.graph)
+    slots, probe = dg.edge_table()
+    assert slots >= 2 * (len(dg.download()[1]) // 2) and probe < 4096
+    dense = [q for q in wl.queries if q.m > q.n - 1]
+    assert dense
+    with_table = [gpu.match(dg, q, cap=100_000) for q in dense]
+    os.environ["GPSM_DEBUG_NO_EDGE_HASH"] = "1"
+    try:
+        lists = [gpu.match(dg, q, cap=100_000) for q in dense]
+    finally:
+        del os.environ["GPSM_DEBUG_NO_EDGE_HASH"]
+    for a, b in zip(with_table, lists):
+        assert a.count == b.count
+        assert np.array_equal(a.pos2id, b.pos2id)
+        assert np.array_equal(a.rows, b.rows)

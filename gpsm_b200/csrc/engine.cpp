@@ -901,9 +901,10 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     R.stats.level_rows[1] = n1;
   }
   bool safe_step = false;  // the next step admits no more candidates than its output holds rows
-  // GPSM_DEBUG_WIDE_STEPS=1: every intermediate step admits 64 times the
-  // candidates its output holds rows, so nearly every step ends at a row
-  // boundary (a test of that path: the rows must not change)
+  // GPSM_DEBUG_WIDE_STEPS=1: every intermediate step admits 16 times the
+  // candidates its output holds rows, so every step that keeps more than a
+  // sixteenth of them ends at a row boundary (a test of that path: the rows
+  // must not change)
   const bool wide_steps = [] {
     const char* e = getenv("GPSM_DEBUG_WIDE_STEPS");
     return e && e[0] == '1';
@@ -982,7 +983,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
       // neighbours' lists reject most) may admit up to out_cap / keep of
       // them; if more rows are kept than out_cap after all, the write pass
       // ends the step at a row boundary and the rest are offered again
-      const double keep = wide_steps ? 1.0 / 64.0 : A.keep;
+      const double keep = wide_steps ? 1.0 / 16.0 : A.keep;
       budget = std::min<uint64_t>(opt.step_cands, safe_step ? out_cap : (uint64_t)((double)out_cap / keep));
       budget = std::max<uint64_t>(budget, std::min<uint64_t>(out_cap, opt.step_cands));
       cut_rows = budget > out_cap;

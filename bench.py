@@ -267,6 +267,13 @@ def reference_build_leg(repeat=20):
 
 def run_ours(args):
     rank, world, local, pg = dist_setup()
+    # every rank is a process with its own pool of page-locked result blocks
+    # (default: a quarter of host memory each): the ranks of this node share
+    # that quarter unless the caller chose a size
+    local_world = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+    if local_world > 1 and "GPSM_HOST_POOL_GB" not in os.environ:
+        ram_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30
+        os.environ["GPSM_HOST_POOL_GB"] = str(max(2.0, min(64.0, ram_gb / 4) / local_world))
     import gpsm_b200 as G
     from gpsm_b200 import workloads as W
     G.init(local)

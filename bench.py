@@ -274,6 +274,10 @@ def run_ours(args):
     if local_world > 1 and "GPSM_HOST_POOL_GB" not in os.environ:
         ram_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30
         os.environ["GPSM_HOST_POOL_GB"] = str(max(2.0, min(64.0, ram_gb / 4) / local_world))
+    # the ranks' slot threads share the host's cores: they sleep while their
+    # GPU works instead of spinning
+    if local_world > 1:
+        os.environ.setdefault("GPSM_BLOCKING_SYNC", "1")
     import gpsm_b200 as G
     from gpsm_b200 import workloads as W
     G.init(local)

@@ -357,7 +357,7 @@ static std::vector<int32_t> learned_order(Workspace& ws, const DeviceGraph& g, c
   std::vector<char> hout(plan_out_bytes() * (starts.size() + 1));
   char* h_plan = reinterpret_cast<char*>(ws.h_small + 2048);  // the plans, through the pinned mirror
   small_to_host(ws, h_plan, d_out, hout.size());
-  GPSM_CUDA(cudaStreamSynchronize(s));
+  stream_wait(ws);
   memcpy(hout.data(), h_plan, hout.size());
   ws.arena.used = mark;  // planner scratch is not needed by the joins
   const size_t ob = plan_out_bytes();
@@ -493,7 +493,7 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
     GPSM_CUDA(cudaMemcpyAsync(d_params, params.data(), params.size() * 4, cudaMemcpyHostToDevice, s));
   uint32_t** d_lists = arena_alloc<uint32_t*>(ws, qn);
   GPSM_CUDA(cudaMemcpyAsync(d_lists, list.data(), qn * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
-  GPSM_CUDA(cudaStreamSynchronize(s));  // params and list are pageable host memory
+  stream_wait(ws);  // params and list are pageable host memory
 
   auto bm_of = [&](uint32_t u) { return bm + (size_t)u * W; };
   uint64_t launches = 0;
@@ -548,7 +548,7 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
   ++launches;
   small_to_host(ws, ws.h_small, counts, qn * sizeof(uint32_t));
   small_to_host(ws, ws.h_small + 64, ws.d_flags, sizeof(uint32_t));
-  GPSM_CUDA(cudaStreamSynchronize(s));
+  stream_wait(ws);
   std::vector<uint32_t> cnt(qn);
   memcpy(cnt.data(), ws.h_small, qn * sizeof(uint32_t));
   const uint32_t flags = *reinterpret_cast<uint32_t*>(ws.h_small + 64);
@@ -606,7 +606,7 @@ static int run_filter(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, M
     launch_gather_u64(ws, goff, d_idx, ndir + 1, ws.d_small);
     small_to_host(ws, ws.h_small, ws.d_small, (ndir + 1) * sizeof(unsigned long long));
     small_to_host(ws, ws.h_small + 4000, ws.d_flags, sizeof(uint32_t));
-    GPSM_CUDA(cudaStreamSynchronize(s));
+    stream_wait(ws);
     if (*reinterpret_cast<uint32_t*>(ws.h_small + 4000) & DF_SCAN_TIMEOUT) {
       set_last_error("device wait limit tripped in candidate-edge scan");
       return GPSM_ERR_TIMEOUT;
@@ -773,7 +773,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
   // zero once: every write pass clears the tile counts it read
   GPSM_CUDA(cudaMemsetAsync(js.tile_cnt, 0, js.tiles * sizeof(uint32_t), s));
   GPSM_CUDA(cudaMemsetAsync(d_st2, 0, 2 * sizeof(StepState), s));
-  GPSM_CUDA(cudaStreamSynchronize(s));  // hb is pageable
+  stream_wait(ws);  // hb is pageable
 
   R.stats.level_rows.assign(qn + 1, 0);
   R.stats.level_in.assign(qn + 1, 0);
@@ -853,7 +853,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     d_checks = arena_alloc<uint32_t>(ws, chk.size() + 1);
     d_kept = arena_alloc<unsigned long long>(ws, 1);
     if (!chk.empty()) GPSM_CUDA(cudaMemcpyAsync(d_checks, chk.data(), chk.size() * 4, cudaMemcpyHostToDevice, s));
-    GPSM_CUDA(cudaStreamSynchronize(s));
+    stream_wait(ws);
   }
   uint64_t res_used = 0, emitted = 0;
   bool capped = false;
@@ -1005,7 +1005,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
     GPSM_CUDA(cudaEventRecord(ws.eve1, s));
     exp_launches += 4;  // locate, check, scan, write
     ++R.stats.join_steps;
-    GPSM_CUDA(cudaStreamSynchronize(s));  // the write pass filled h_st
+    stream_wait(ws);  // the write pass filled h_st
     {
       float ems = 0;
       GPSM_CUDA(cudaEventElapsedTime(&ems, ws.eve0, ws.eve1));
@@ -1063,7 +1063,7 @@ static int join_attempt(JoinContext& C, uint64_t limit, bool& hit_limit) {
       launch_verify_directed(ws, stage, written, qn, d_checks, nchecks, g.dir_off, g.dir_col, g.dir_lab,
                              res_buf + res_used * qn, d_kept);
       small_to_host(ws, &h_st->verified, d_kept, sizeof(unsigned long long));
-      GPSM_CUDA(cudaStreamSynchronize(s));
+      stream_wait(ws);
       kept = std::min<uint64_t>(h_st->verified, cap - emitted);  // the cap counts rows that pass
       ++exp_launches;
     }
@@ -1115,7 +1115,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   if (ws.dirty) {
     // an earlier query stopped part-way: re-read the scan ticket counter so
     // the host's per-launch ticket base matches the device again
-    GPSM_CUDA(cudaStreamSynchronize(s));
+    stream_wait(ws);
     GPSM_CUDA(cudaMemcpy(&ws.scan.ticket_base, ws.scan.d_ticket, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   }
   ws.dirty = true;
@@ -1168,7 +1168,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   for (uint32_t p = 0; p < qn; ++p) R.id2pos[pos2id[p]] = (int32_t)p;
   GPSM_CUDA(cudaEventRecord(ws.evm, s));
   if (opt.filter_only) {
-    GPSM_CUDA(cudaStreamSynchronize(s));
+    stream_wait(ws);
     return GPSM_OK;
   }
   // join memory: level buffers, step scratch and the result buffer are the
@@ -1250,7 +1250,7 @@ int run_query(Workspace& ws, const DeviceGraph& g, const QueryPlan& Q, const Mat
   if (jrc != GPSM_OK) return jrc;
   small_to_host(ws, ws.h_small + 4001, ws.d_flags, sizeof(uint32_t));
   GPSM_CUDA(cudaEventSynchronize(ws.ev1));
-  GPSM_CUDA(cudaStreamSynchronize(s));
+  stream_wait(ws);
   if (*reinterpret_cast<uint32_t*>(ws.h_small + 4001) & (DF_SCAN_TIMEOUT | DF_BOUNDS)) {
     set_last_error("device wait limit or bounds check tripped in the joins");
     return GPSM_ERR_TIMEOUT;

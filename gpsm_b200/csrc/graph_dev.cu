@@ -362,6 +362,7 @@ void workspace_free(Workspace* ws) {
     if (ws->ev_res[i]) cudaEventDestroy(ws->ev_res[i]);
     if (ws->ev_copied[i]) cudaEventDestroy(ws->ev_copied[i]);
   }
+  if (ws->ev_block) cudaEventDestroy(ws->ev_block);
   cudaFree(ws->arena.base);
   cudaFree(ws->scan.d_ticket);
   cudaFree(ws->scan.d_status);

@@ -259,6 +259,20 @@ bool HostRows::append_from_device_async(Workspace& ws, const uint32_t* d_src, ui
   return true;
 }
 
+void stream_wait(Workspace& ws) {
+  static const bool blocking = [] {
+    const char* e = getenv("GPSM_BLOCKING_SYNC");
+    return e && e[0] == '1';
+  }();
+  if (!blocking) {
+    GPSM_CUDA(cudaStreamSynchronize(ws.stream));
+    return;
+  }
+  if (!ws.ev_block) GPSM_CUDA(cudaEventCreateWithFlags(&ws.ev_block, cudaEventDisableTiming | cudaEventBlockingSync));
+  GPSM_CUDA(cudaEventRecord(ws.ev_block, ws.stream));
+  GPSM_CUDA(cudaEventSynchronize(ws.ev_block));
+}
+
 void copy_to_host(Workspace& ws, uint32_t* dst, const uint32_t* d_src, uint64_t words) {
   if (words == 0) return;
   cudaStream_t s = ws.stream;

@@ -177,6 +177,7 @@ struct Workspace {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_res[2] = {nullptr, nullptr};     // buffer k written (on stream)
   cudaEvent_t ev_copied[2] = {nullptr, nullptr};  // buffer k copied out (on copy_stream)
+  cudaEvent_t ev_block = nullptr;  // stream_wait's sleeping event (created at first use)
   // Two result buffers that outlive a query (carved once from the top of
   // the arena, which shrinks by their size): a query's last copies out of
   // them may still run while the slot's next query starts; its joins wait
@@ -197,6 +198,12 @@ struct Workspace {
     return true;
   }
 };
+
+// Waits for everything queued on ws.stream. With GPSM_BLOCKING_SYNC=1 the
+// thread sleeps on an event created with cudaEventBlockingSync instead of
+// spinning: many slot threads in several processes (one per GPU) on a few
+// host cores would otherwise spin one another off the cores.
+void stream_wait(Workspace& ws);
 
 // Copies `words` 32-bit words from device memory to pageable host memory
 // through the workspace's pinned staging buffers, on the workspace stream;

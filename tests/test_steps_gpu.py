@@ -54,3 +54,33 @@ def test_edge_table_and_list_search_give_the_same_rows(gpu):
         assert a.count == b.count
         assert np.array_equal(a.pos2id, b.pos2id)
         assert np.array_equal(a.rows, b.rows)
+
+
+_CHILD = """
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import gpsm_b200 as G
+from gpsm_b200 import workloads as W
+G.init(0)
+wl = W.workload("rmat20_mix", count=4)
+dg = G.DeviceGraph(wl.graph)
+rows = [G.match(dg, q, cap=20_000, work_cap=10**10).rows for q in wl.queries]
+np.save(sys.argv[2], np.concatenate([r.ravel() for r in rows]))
+"""
+
+
+def test_blocking_sync_mode_gives_the_same_rows(gpu, tmp_path):
+    """GPSM_BLOCKING_SYNC=1 (threads sleep on an event while their stream
+    works; read once per process, so a child process runs it) returns the
+    same rows as the default waits."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = []
+    for mode in ("0", "1"):
+        path = str(tmp_path / f"rows{mode}.npy")
+        env = dict(os.environ, GPSM_BLOCKING_SYNC=mode)
+        subprocess.run([sys.executable, "-c", _CHILD, root, path], env=env, check=True, timeout=600)
+        outs.append(np.load(path))
+    assert outs[0].size > 0 and np.array_equal(outs[0], outs[1])

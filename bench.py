@@ -265,19 +265,27 @@ def reference_build_leg(repeat=20):
             "ours_exe": "gpsm_b200/gpsm_run"}
 
 
+def rank_host_settings(local_world, environ, ram_gb):
+    """Environment a rank sets before the library starts when `local_world`
+    ranks share this host: every rank is a process with its own pool of
+    page-locked result blocks (default: a quarter of host memory each), so
+    they share that quarter unless the caller chose a size; and their slot
+    threads share the host's cores, so they sleep while their GPU works
+    instead of spinning."""
+    out = {}
+    if local_world > 1:
+        if "GPSM_HOST_POOL_GB" not in environ:
+            out["GPSM_HOST_POOL_GB"] = str(max(2.0, min(64.0, ram_gb / 4) / local_world))
+        if "GPSM_BLOCKING_SYNC" not in environ:
+            out["GPSM_BLOCKING_SYNC"] = "1"
+    return out
+
+
 def run_ours(args):
     rank, world, local, pg = dist_setup()
-    # every rank is a process with its own pool of page-locked result blocks
-    # (default: a quarter of host memory each): the ranks of this node share
-    # that quarter unless the caller chose a size
     local_world = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
-    if local_world > 1 and "GPSM_HOST_POOL_GB" not in os.environ:
-        ram_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30
-        os.environ["GPSM_HOST_POOL_GB"] = str(max(2.0, min(64.0, ram_gb / 4) / local_world))
-    # the ranks' slot threads share the host's cores: they sleep while their
-    # GPU works instead of spinning
-    if local_world > 1:
-        os.environ.setdefault("GPSM_BLOCKING_SYNC", "1")
+    ram_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2**30
+    os.environ.update(rank_host_settings(local_world, os.environ, ram_gb))
     import gpsm_b200 as G
     from gpsm_b200 import workloads as W
     G.init(local)

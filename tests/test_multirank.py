@@ -62,3 +62,17 @@ def test_reference_arm_prints_one_json_line_without_the_engine():
     assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0
     assert "MAPPED False" in out.stdout
+
+
+def test_ranks_on_one_host_share_the_page_locked_pool_and_sleep_in_waits():
+    """Eight ranks on a host with 256 GiB: each gets an eighth of the default
+    pool (a quarter of host memory) and sleeping waits; a caller's own
+    choices stand; a single rank keeps the library defaults."""
+    sys.path.insert(0, ROOT)
+    import bench
+    s = bench.rank_host_settings(8, {}, 256.0)
+    assert s == {"GPSM_HOST_POOL_GB": str(64.0 / 8), "GPSM_BLOCKING_SYNC": "1"}
+    s = bench.rank_host_settings(8, {"GPSM_HOST_POOL_GB": "3", "GPSM_BLOCKING_SYNC": "0"}, 256.0)
+    assert s == {}
+    assert bench.rank_host_settings(1, {}, 256.0) == {}
+    assert float(bench.rank_host_settings(64, {}, 64.0)["GPSM_HOST_POOL_GB"]) == 2.0  # at least 2 GiB each

@@ -22,6 +22,8 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <new>
+#include <stdexcept>
 #include <thread>
 
 #include "engine.h"
@@ -136,6 +138,12 @@ int run_batch_parallel(SlotPool& pool, const DeviceGraph& g, uint32_t nq, const 
         }
       } catch (const CudaError& e) {
         rc = e.err == cudaErrorMemoryAllocation ? GPSM_ERR_NOMEM : GPSM_ERR_CUDA;
+      } catch (const std::bad_alloc&) {
+        set_last_error("batch slot: host allocation failed");
+        rc = GPSM_ERR_NOMEM;
+      } catch (const std::exception& e) {
+        set_last_error(std::string("batch slot: ") + e.what());
+        rc = GPSM_ERR_CUDA;
       }
       out.status[k] = rc;
       if (rc != GPSM_OK) {
@@ -293,6 +301,12 @@ struct Server {
         }
       } catch (const CudaError& e) {
         rc = e.err == cudaErrorMemoryAllocation ? GPSM_ERR_NOMEM : GPSM_ERR_CUDA;
+      } catch (const std::bad_alloc&) {
+        set_last_error("server slot: host allocation failed");
+        rc = GPSM_ERR_NOMEM;
+      } catch (const std::exception& e) {
+        set_last_error(std::string("server slot: ") + e.what());
+        rc = GPSM_ERR_CUDA;
       }
       if (R.copies_done && rc != GPSM_OK) {  // no request takes the rows: let the copies end here
         cudaEventSynchronize(R.copies_done);
